@@ -1,0 +1,367 @@
+"""Benchmark of the gridding / degridding hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--precision mixed|fp64] [--nvis 10000000]
+
+Workload (one "step"): degrid_grid_visibilities of one batch of 10M
+four-polarization visibilities onto a 2048x2048x4x1 complex128 grid with a
+dense 4x4 Mueller matrix (16 CF planes), 8 w-plane CF groups with supports
+8..32 (9..33 taps) at oversampling 128, starting from a complex128 N(0,1)
+model.  All inputs are seeded synthetic data with those shapes.
+
+Printed (rank 0, one JSON line): Mvis/s with inputs resident in HBM
+("value"), the same through the public API with pinned host input and a
+device->host read of the weights ("e2e"), the HBM roofline of the step, the
+CPU baseline (threaded CPU restatement on a bounded sample) and the SM clocks
+sampled during the timed region.
+
+Under torchrun (N > 1) every rank runs its own replica of the workload on its
+GPU (weak scaling); the step time is the maximum over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mvis/s grid+degrid (degrid_grid_visibilities), 2048^2x4 pol, 10M vis"
+UNIT = "Mvis/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--precision", default="fp64", choices=["mixed", "fp64"])
+    p.add_argument("--nvis", type=int, default=10_000_000)
+    p.add_argument("--grid", type=int, default=2048)
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"),
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def make_workload(args, seed_offset, device):
+    import torch
+    from hpg_b200 import workloads
+    p = workloads.full_pol_params(supports=workloads.FULL_POL_SUPPORTS,
+                                  oversampling=128, seed=20261204 + seed_offset)
+    rng = p["rng"]
+    grid_size = (args.grid, args.grid, 4, 1)
+    vis = workloads.visibilities(args.nvis, 4, grid_size, p["grid_scale"],
+                                 p["freq"], rng, w_frac=0.3,
+                                 ngroups=len(p["supports"]))
+    ext, vals = workloads.separable_cf_torch(p["supports"], p["oversampling"],
+                                             p["mueller_factors"], device,
+                                             w_phases=p["w_phases"])
+    g = torch.Generator(device=device).manual_seed(7 + seed_offset)
+    model = torch.complex(
+        torch.randn((1, 4, args.grid, args.grid), generator=g, device=device,
+                    dtype=torch.float64),
+        torch.randn((1, 4, args.grid, args.grid), generator=g, device=device,
+                    dtype=torch.float64))
+    return dict(p=p, grid_size=grid_size, vis=vis, cf_extents=ext,
+                cf_values=vals, model=model)
+
+
+def taps_of(supports):
+    return [s + 1 if s % 2 == 0 else s for s in supports]
+
+
+def cpu_baseline(wl, target_s, nthreads=None):
+    """Threaded CPU restatement (oracle) of the same step on a bounded
+    sample of the same visibilities; returns (Mvis/s, sample, threads)."""
+    from oracle import oracle as O
+    p = wl["p"]
+    nthreads = nthreads or O.num_threads()
+    cf_host = [v.cpu().numpy() for v in wl["cf_values"]]
+    model = wl["model"].cpu().numpy()
+    o = O.Oracle(wl["grid_size"], p["grid_scale"], p["mueller"],
+                 p["conj_mueller"], p["oversampling"], wl["cf_extents"],
+                 cf_host)
+    o.set_model(model)
+    vis = wl["vis"]
+    n = 2000
+    t0 = time.perf_counter()
+    o.grid_visibilities(vis[:n], do_degrid=True, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    n2 = int(min(len(vis) - n, max(n, target_s / max(dt / n, 1e-9))))
+    t0 = time.perf_counter()
+    o.grid_visibilities(vis[n:n + n2], do_degrid=True, nthreads=nthreads)
+    dt2 = time.perf_counter() - t0
+    return n2 / dt2 / 1e6, n2, dt2, nthreads
+
+
+def run_reference(args, rank):
+    """The reference's CPU implementation of the path (its Kokkos
+    Serial/OpenMP build is not buildable here: the CPU restatement stands in)
+    on the host cores, on this arm's workload and metric."""
+    if rank != 0:
+        return
+    import torch
+    from oracle import oracle as O
+    dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
+    wl = make_workload(args, 0, dev)
+    nthreads = O.num_threads()
+    p = wl["p"]
+    cf_host = [v.cpu().numpy() for v in wl["cf_values"]]
+    model = wl["model"].cpu().numpy()
+    del wl["cf_values"]
+    o = O.Oracle(wl["grid_size"], p["grid_scale"], p["mueller"],
+                 p["conj_mueller"], p["oversampling"], wl["cf_extents"], cf_host)
+    o.set_model(model)
+    vis = wl["vis"]
+    # bounded sample per step: ~args.cpu_seconds / (warmup + steps)
+    n = 1000
+    t0 = time.perf_counter()
+    o.grid_visibilities(vis[:n], do_degrid=True, nthreads=nthreads)
+    per_vis = (time.perf_counter() - t0) / n
+    per_step = max(2.0, 60.0 / max(args.steps + args.warmup, 1))
+    n_step = int(max(1000, min(len(vis), per_step / per_vis)))
+    off = n
+    for _ in range(args.warmup):
+        o.grid_visibilities(vis[off:off + n_step], do_degrid=True, nthreads=nthreads)
+        off = (off + n_step) % max(len(vis) - n_step, 1)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.grid_visibilities(vis[off:off + n_step], do_degrid=True, nthreads=nthreads)
+        times.append(time.perf_counter() - t0)
+        off = (off + n_step) % max(len(vis) - n_step, 1)
+    value = n_step * len(times) / sum(times) / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "full-pol degrid+grid 2048x2048x4, 8 CF groups "
+                               "(supports 8-32, os 128), dense 4x4 Mueller",
+                   "nvis": args.nvis, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads,
+                         "kind": "port",
+                         "sample": f"{n_step} visibilities per step of the "
+                                   f"{args.nvis}-visibility batch"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    import hpg_b200
+    from hpg_b200 import CFArray, Gridder, workloads
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=dev)
+    hpg_b200.load()
+
+    wl = make_workload(args, rank, dev)
+    p = wl["p"]
+    g = Gridder.create(local_rank, 0, args.nvis, None, wl["grid_size"],
+                       p["grid_scale"], p["mueller"], p["conj_mueller"])
+    g.set_precision(hpg_b200.PRECISION_MIXED if args.precision == "mixed"
+                    else hpg_b200.PRECISION_FP64)
+    g.set_convolution_function(CFArray(p["oversampling"], wl["cf_extents"],
+                                       wl["cf_values"]), on_device=True)
+    g.set_model(wl["model"], on_device=True)
+    cpu_wl = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu_wl = wl
+    else:
+        del wl["cf_values"]
+        torch.cuda.empty_cache()
+
+    vis = wl["vis"]
+    dvis = torch.from_numpy(vis.view(np.uint8)).to(dev)
+    hvis = torch.from_numpy(vis.view(np.uint8)).pin_memory()
+    hvis_np = hvis.numpy().view(vis.dtype)
+    stream = torch.cuda.ExternalStream(g.stream, device=dev)
+
+    def step_device():
+        g.degrid_grid_visibilities(dvis, on_device=True)
+
+    def step_e2e():
+        g.degrid_grid_visibilities(hvis_np)
+        return g.grid_weights()
+
+    for _ in range(args.warmup):
+        step_device()
+    g.fence()
+
+    def timed(fn, k):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        g.fence()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(k):
+            fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        g.fence()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        return ms
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = g.kernel_launches()
+    ms = timed(step_device, args.steps)
+    launches = g.kernel_launches() - launches0
+    clock_summary = clocks.stop()
+
+    for _ in range(1):
+        step_e2e()
+    ms_e2e = timed(step_e2e, max(1, min(args.steps, 3)))
+    e2e_steps = max(1, min(args.steps, 3))
+
+    ms_step = ms / args.steps
+    total_vis = args.nvis * world
+    value = total_vis / (ms_step * 1e-3) / 1e6
+    e2e_value = total_vis / (ms_e2e / e2e_steps * 1e-3) / 1e6
+
+    taps = taps_of(p["supports"])
+    b_alg = workloads.algorithmic_bytes(vis, 4, taps, 16,
+                                        int(np.prod(wl["grid_size"])), 3)
+    peak, peak_kind = peaks()
+    achieved = b_alg / (ms_step * 1e-3) / 1e9
+
+    cpu = None
+    if cpu_wl is not None:
+        try:
+            v, n, dt, nt = cpu_baseline(cpu_wl, args.cpu_seconds)
+            cpu = {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
+                   "sample": f"{n} visibilities of the same batch "
+                             f"({dt:.1f} s, threaded CPU restatement)"}
+        except Exception as e:  # reported, not hidden
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32-mixed",
+            "data": "synthetic",
+            "config": {
+                "workload": "full-pol degrid+grid 2048x2048x4, 8 CF groups "
+                            "(supports 8-32, os 128), dense 4x4 Mueller",
+                "nvis": args.nvis, "grid": list(wl["grid_size"]),
+                "precision": args.precision,
+                "l2": "inputs larger than L2 (CF 10 GB, visibilities 1.2 GB)",
+                "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": int(vis.nbytes),
+                    "d2h_bytes_per_step": int(np.prod(wl["grid_size"][2:]) * 8)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_step": b_alg},
+            "cpu_baseline": cpu,
+            "clocks": clock_summary,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

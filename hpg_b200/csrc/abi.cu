@@ -1,0 +1,605 @@
+// abi.cu -- the extern "C" entry points of libhpgb.so (include/hpgb.h).
+//
+// Each entry point replaces one virtual of hpg::runtime::State
+// (src/hpg_runtime.hpp:80-207) as implemented by StateT<Device::Cuda>
+// (src/hpg_runtime.hpp:721-1750); the header names the virtual for each.
+
+#include <algorithm>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "gridder.cuh"
+
+namespace hpgb {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+Status grid_batch(hpgb_gridder* g, const void* d_vis, size_t n,
+                  unsigned flags);  // grid_tiled.cu
+
+namespace {
+
+int finish(const Status& s) {
+  if (!s) set_last_error(s.msg);
+  else set_last_error("");
+  return s.code;
+}
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    return finish(f());
+  } catch (const std::bad_alloc&) {
+    return finish(Status::err(HPGB_ERROR_OTHER, "host allocation failed"));
+  } catch (const std::exception& e) {
+    return finish(Status::err(HPGB_ERROR_OTHER, e.what()));
+  } catch (...) {
+    return finish(Status::err(HPGB_ERROR_OTHER, "unknown exception"));
+  }
+}
+
+Status check_status_word(hpgb_gridder* g) {
+  // status word lives in the first bytes of vb.counters
+  unsigned h = 0;
+  if (!g->vb.counters.ptr) return Status::ok();
+  HPGB_CUDA_TRY(cudaMemcpy(&h, g->vb.counters.ptr, sizeof(unsigned),
+                           cudaMemcpyDeviceToHost));
+  if (h & kStatusBadIndex) {
+    HPGB_CUDA_TRY(cudaMemsetAsync(g->vb.counters.ptr, 0, sizeof(unsigned),
+                                  g->stream));
+    HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    return Status::err(HPGB_ERROR_OUT_OF_BOUNDS_CF_INDEX,
+                       "visibility cf_index or grid_cube out of bounds; "
+                       "the visibility was skipped");
+  }
+  return Status::ok();
+}
+
+Status fence_impl(const hpgb_gridder* cg) {
+  hpgb_gridder* g = const_cast<hpgb_gridder*>(cg);
+  HPGB_CUDA_TRY(cudaSetDevice(g->device));
+  HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  g->pending_dst = nullptr;
+  g->pending_bytes = 0;
+  return check_status_word(g);
+}
+
+Status alloc_grid(hpgb_gridder* g, bool zero_weights) {
+  HPGB_TRY(g->grid.reserve(std::max<size_t>(g->grid_elems(), 1) * sizeof(double2)));
+  HPGB_CUDA_TRY(cudaMemsetAsync(g->grid.ptr, 0, g->grid_elems() * sizeof(double2),
+                                g->stream));
+  if (zero_weights) {
+    HPGB_TRY(g->weights.reserve(std::max<size_t>(g->weight_elems(), 1) * sizeof(double)));
+    HPGB_CUDA_TRY(cudaMemsetAsync(g->weights.ptr, 0,
+                                  g->weight_elems() * sizeof(double), g->stream));
+  }
+  return Status::ok();
+}
+
+// host-side index validation (the check the reference leaves commented out,
+// src/hpg_runtime.hpp:1093-1100)
+template <int N>
+Status validate_host_indexes(const hpgb_gridder* g, const void* vis, size_t n) {
+  const VisData<N>* v = static_cast<const VisData<N>*>(vis);
+  const CFRegion& cf = g->cf;
+  for (size_t i = 0; i < n; ++i) {
+    const unsigned grp = v[i].cf_index[1], cube = v[i].cf_index[0];
+    if (grp >= cf.extents.size() || cube >= cf.extents[grp][3] ||
+        v[i].grid_cube >= g->grid_size[3])
+      return Status::err(
+          HPGB_ERROR_OUT_OF_BOUNDS_CF_INDEX,
+          "visibility " + std::to_string(i) + ": cf_index (" +
+              std::to_string(cube) + "," + std::to_string(grp) +
+              ") or grid_cube " + std::to_string(v[i].grid_cube) +
+              " is out of bounds");
+  }
+  return Status::ok();
+}
+
+Status validate_indexes(const hpgb_gridder* g, const void* vis, size_t n) {
+  switch (g->npol) {
+    case 1: return validate_host_indexes<1>(g, vis, n);
+    case 2: return validate_host_indexes<2>(g, vis, n);
+    case 3: return validate_host_indexes<3>(g, vis, n);
+    case 4: return validate_host_indexes<4>(g, vis, n);
+    default: return Status::err(HPGB_ERROR_OTHER, "bad polarization count");
+  }
+}
+
+// every Mueller index must address a Mueller plane of every CF group (the
+// reference indexes the CF view without a check, src/hpg_core.hpp:656, :865)
+Status validate_mueller(const hpgb_gridder* g) {
+  int max_index = -1;
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c)
+      max_index = std::max(max_index, std::max(g->mt.m[r][c], g->mt.c[r][c]));
+  for (size_t grp = 0; grp < g->cf.groups.size(); ++grp)
+    if (max_index >= g->cf.groups[grp].nmueller)
+      return Status::err(HPGB_ERROR_OTHER,
+                         "Mueller index " + std::to_string(max_index) +
+                             " exceeds the Mueller extent of CF group " +
+                             std::to_string(grp));
+  return Status::ok();
+}
+
+}  // namespace
+}  // namespace hpgb
+
+using namespace hpgb;
+
+hpgb::GridGeom hpgb_gridder::geom() const {
+  GridGeom g;
+  g.nx = int(grid_size[0]);
+  g.ny = int(grid_size[1]);
+  g.nrow = int(grid_size[2]);
+  g.ncube = int(grid_size[3]);
+  g.scale_x = grid_scale[0];
+  g.scale_y = grid_scale[1];
+  g.os = int(cf.os);
+  g.nfine = 2 * int(cf.os / 2) + 1;
+  g.ngroups = int(cf.groups.size());
+  g.mt = mt;
+  g.status = vb.counters.as<unsigned>();
+  return g;
+}
+
+extern "C" {
+
+int hpgb_abi_version(void) { return HPGB_ABI_VERSION; }
+
+const char* hpgb_last_error_message(void) { return g_last_error.c_str(); }
+
+int hpgb_device_count(int* count) {
+  return guarded([&]() -> Status {
+    if (!count) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      c = 0;
+    }
+    *count = c;
+    return Status::ok();
+  });
+}
+
+int hpgb_create(int device_id, unsigned max_added_tasks,
+                size_t max_visibility_batch_size, const unsigned grid_size[4],
+                const double grid_scale[2], unsigned num_polarizations,
+                const int* mueller_indexes,
+                const int* conjugate_mueller_indexes, hpgb_gridder** out) {
+  return guarded([&]() -> Status {
+    if (!out || !grid_size || !grid_scale || !mueller_indexes ||
+        !conjugate_mueller_indexes)
+      return Status::err(HPGB_ERROR_OTHER, "null argument");
+    *out = nullptr;
+    if (num_polarizations < 1 || num_polarizations > 4)
+      return Status::err(HPGB_ERROR_INVALID_NUMBER_POLARIZATIONS,
+                         "number of polarizations must be 1..4");
+    if (grid_size[2] < 1 || grid_size[2] > 4)
+      return Status::err(HPGB_ERROR_INVALID_NUMBER_MUELLER_INDEX_ROWS,
+                         "number of Mueller index rows must be 1..4");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+      cudaGetLastError();
+      count = 0;
+    }
+    const int dev = device_id < 0 ? 0 : device_id;
+    if (dev >= count)
+      return Status::err(HPGB_ERROR_DISABLED_DEVICE,
+                         "Requested device is not enabled");
+    HPGB_CUDA_TRY(cudaSetDevice(dev));
+    std::unique_ptr<hpgb_gridder> g(new hpgb_gridder);
+    g->device = dev;
+    g->max_added_tasks = max_added_tasks;
+    g->max_batch = max_visibility_batch_size;
+    std::copy(grid_size, grid_size + 4, g->grid_size);
+    std::copy(grid_scale, grid_scale + 2, g->grid_scale);
+    g->npol = num_polarizations;
+    for (int r = 0; r < 4; ++r)
+      for (int c = 0; c < 4; ++c) {
+        const bool in = r < int(grid_size[2]) && c < int(num_polarizations);
+        g->mt.m[r][c] = in ? mueller_indexes[r * num_polarizations + c] : -1;
+        g->mt.c[r][c] = in ? conjugate_mueller_indexes[r * num_polarizations + c] : -1;
+      }
+    HPGB_CUDA_TRY(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    HPGB_TRY(g->vb.counters.reserve(256));
+    HPGB_CUDA_TRY(cudaMemsetAsync(g->vb.counters.ptr, 0, 256, g->stream));
+    HPGB_TRY(alloc_grid(g.get(), true));
+    HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    *out = g.release();
+    return Status::ok();
+  });
+}
+
+int hpgb_clone(const hpgb_gridder* src, hpgb_gridder** out) {
+  return guarded([&]() -> Status {
+    if (!src || !out) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    *out = nullptr;
+    HPGB_TRY(fence_impl(src));
+    std::unique_ptr<hpgb_gridder> g(new hpgb_gridder);
+    g->device = src->device;
+    g->max_added_tasks = src->max_added_tasks;
+    g->max_batch = src->max_batch;
+    std::copy(src->grid_size, src->grid_size + 4, g->grid_size);
+    std::copy(src->grid_scale, src->grid_scale + 2, g->grid_scale);
+    g->npol = src->npol;
+    g->mt = src->mt;
+    g->precision = src->precision;
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    HPGB_CUDA_TRY(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    HPGB_TRY(g->vb.counters.reserve(256));
+    HPGB_CUDA_TRY(cudaMemsetAsync(g->vb.counters.ptr, 0, 256, g->stream));
+    HPGB_TRY(g->grid.reserve(src->grid.bytes));
+    HPGB_CUDA_TRY(cudaMemcpyAsync(g->grid.ptr, src->grid.ptr, src->grid.bytes,
+                                  cudaMemcpyDeviceToDevice, g->stream));
+    HPGB_TRY(g->weights.reserve(src->weights.bytes));
+    HPGB_CUDA_TRY(cudaMemcpyAsync(g->weights.ptr, src->weights.ptr,
+                                  src->weights.bytes, cudaMemcpyDeviceToDevice,
+                                  g->stream));
+    if (src->has_model) {
+      HPGB_TRY(g->model.reserve(src->model.bytes));
+      HPGB_CUDA_TRY(cudaMemcpyAsync(g->model.ptr, src->model.ptr,
+                                    src->model.bytes, cudaMemcpyDeviceToDevice,
+                                    g->stream));
+      g->has_model = true;
+    }
+    HPGB_TRY(copy_cf(g.get(), src));
+    HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    *out = g.release();
+    return Status::ok();
+  });
+}
+
+int hpgb_destroy(hpgb_gridder* g) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::ok();
+    cudaSetDevice(g->device);
+    cudaStreamSynchronize(g->stream);
+    release_fft_plans(g);
+    cudaStream_t s = g->stream;
+    delete g;  // DevBuf destructors free device memory
+    if (s) cudaStreamDestroy(s);
+    return Status::ok();
+  });
+}
+
+int hpgb_set_precision(hpgb_gridder* g, int precision) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    if (precision != HPGB_PRECISION_FP64 && precision != HPGB_PRECISION_MIXED)
+      return Status::err(HPGB_ERROR_OTHER, "unknown precision");
+    g->precision = precision;
+    return Status::ok();
+  });
+}
+
+int hpgb_get_stream(const hpgb_gridder* g, void** stream) {
+  return guarded([&]() -> Status {
+    if (!g || !stream) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    *stream = static_cast<void*>(g->stream);
+    return Status::ok();
+  });
+}
+
+int hpgb_cf_region_size(const hpgb_gridder* g, unsigned os, unsigned ngroups,
+                        const unsigned* extents, size_t* bytes) {
+  return guarded([&]() -> Status {
+    if (!bytes) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    if (ngroups == 0 || !extents) {
+      *bytes = g ? g->cf.data.bytes + g->cf.wsum.bytes : 0;
+      return Status::ok();
+    }
+    if (os == 0) return Status::err(HPGB_ERROR_OTHER, "oversampling must be > 0");
+    size_t d = 0, w = 0;
+    HPGB_TRY(cf_region_bytes(os, ngroups, extents, &d, &w));
+    *bytes = d + w;
+    return Status::ok();
+  });
+}
+
+int hpgb_allocate_cf_region(hpgb_gridder* g, unsigned os, unsigned ngroups,
+                            const unsigned* extents) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    HPGB_TRY(fence_impl(g));
+    if (ngroups == 0 || !extents) return Status::ok();
+    if (os == 0) return Status::err(HPGB_ERROR_OTHER, "oversampling must be > 0");
+    size_t d = 0, w = 0;
+    HPGB_TRY(cf_region_bytes(os, ngroups, extents, &d, &w));
+    HPGB_TRY(g->cf.data.reserve(std::max<size_t>(d, 16)));
+    HPGB_TRY(g->cf.wsum.reserve(std::max<size_t>(w, 16)));
+    return Status::ok();
+  });
+}
+
+int hpgb_set_cf(hpgb_gridder* g, unsigned os, unsigned ngroups,
+                const unsigned* extents, const void* const* values, int layout,
+                int values_on_device) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    if (ngroups > 0 && (!extents || !values))
+      return Status::err(HPGB_ERROR_OTHER, "null argument");
+    return set_cf(g, os, ngroups, extents, values, layout, values_on_device != 0);
+  });
+}
+
+int hpgb_set_model(hpgb_gridder* g, const void* values, const unsigned ext[4],
+                   int layout, int on_device) {
+  return guarded([&]() -> Status {
+    if (!g || !values || !ext) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    if (!std::equal(ext, ext + 4, g->grid_size))
+      return Status::err(
+          HPGB_ERROR_INVALID_MODEL_GRID_SIZE,
+          "model grid size [" + std::to_string(ext[0]) + "," +
+              std::to_string(ext[1]) + "," + std::to_string(ext[2]) + "," +
+              std::to_string(ext[3]) + "] is different from visibility grid size [" +
+              std::to_string(g->grid_size[0]) + "," + std::to_string(g->grid_size[1]) +
+              "," + std::to_string(g->grid_size[2]) + "," +
+              std::to_string(g->grid_size[3]) + "]");
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    HPGB_TRY(fence_impl(g));
+    const size_t n = g->grid_elems();
+    HPGB_TRY(g->model.reserve(std::max<size_t>(n, 1) * sizeof(double2)));
+    if (layout == HPGB_LAYOUT_LEFT) {
+      HPGB_CUDA_TRY(cudaMemcpyAsync(g->model.ptr, values, n * sizeof(double2),
+                                    on_device ? cudaMemcpyDeviceToDevice
+                                              : cudaMemcpyHostToDevice,
+                                    g->stream));
+    } else {
+      DevBuf tmp;
+      const void* src = values;
+      if (!on_device) {
+        HPGB_TRY(tmp.reserve(n * sizeof(double2)));
+        HPGB_CUDA_TRY(cudaMemcpyAsync(tmp.ptr, values, n * sizeof(double2),
+                                      cudaMemcpyHostToDevice, g->stream));
+        src = tmp.ptr;
+      }
+      HPGB_TRY(to_layout(g, static_cast<const double2*>(src),
+                         g->model.as<double2>(), layout, true, g->grid_size));
+      HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    }
+    HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    g->has_model = true;
+    return Status::ok();
+  });
+}
+
+int hpgb_grid_visibilities(hpgb_gridder* g, const void* vis, size_t n,
+                           unsigned npol, unsigned flags, int vis_on_device,
+                           void* returned) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    // validation order of src/hpg_runtime.hpp:1816-1828
+    if (n > g->max_batch)
+      return Status::err(HPGB_ERROR_EXCESSIVE_NUMBER_VISIBILITIES,
+                         "Number of visibilities exceeds maximum batch size");
+    if (npol != g->npol)
+      return Status::err(HPGB_ERROR_INVALID_NUMBER_POLARIZATIONS,
+                         "Number of visibility polarizations does not match "
+                         "Mueller matrix");
+    const bool do_grid = flags & HPGB_DO_GRID;
+    if (!do_grid && (flags & HPGB_UPDATE_GRID_WEIGHTS))
+      return Status::err(HPGB_ERROR_UPDATE_WEIGHTS_WITHOUT_GRIDDING,
+                         "Unable to update grid weights during degridding only");
+    if (n == 0) return Status::ok();
+    if (!vis) return Status::err(HPGB_ERROR_OTHER, "null visibilities");
+    if ((flags & HPGB_RETURN_VISIBILITIES) && !returned)
+      return Status::err(HPGB_ERROR_OTHER, "null buffer for returned visibilities");
+    if (!g->cf.set)
+      return Status::err(HPGB_ERROR_OTHER, "no convolution function set");
+    HPGB_TRY(validate_mueller(g));
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    if (!vis_on_device) HPGB_TRY(validate_indexes(g, vis, n));
+    const size_t rec = visdata_size(npol);
+    const size_t bytes = n * rec;
+    HPGB_TRY(g->vb.vis.reserve(g->max_batch * rec));
+    HPGB_CUDA_TRY(cudaMemcpyAsync(
+        g->vb.vis.ptr, vis, bytes,
+        vis_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+        g->stream));
+    HPGB_TRY(grid_batch(g, g->vb.vis.ptr, n, flags));
+    if (flags & HPGB_RETURN_VISIBILITIES) {
+      HPGB_CUDA_TRY(cudaMemcpyAsync(
+          returned, g->vb.vis.ptr, bytes,
+          vis_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+          g->stream));
+      g->pending_dst = returned;
+      g->pending_bytes = bytes;
+      g->pending_on_device = vis_on_device != 0;
+    }
+    return Status::ok();
+  });
+}
+
+int hpgb_fence(const hpgb_gridder* g) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    return fence_impl(g);
+  });
+}
+
+int hpgb_copy_weights(const hpgb_gridder* cg, double* dst, int layout) {
+  return guarded([&]() -> Status {
+    if (!cg || !dst) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    hpgb_gridder* g = const_cast<hpgb_gridder*>(cg);
+    HPGB_TRY(fence_impl(g));
+    std::vector<double> h(g->weight_elems());
+    HPGB_CUDA_TRY(cudaMemcpy(h.data(), g->weights.ptr, h.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost));
+    return weights_to_layout(g, h.data(), dst, layout);
+  });
+}
+
+static Status copy_values(hpgb_gridder* g, const DevBuf& buf, bool present,
+                          void* dst, int layout) {
+  HPGB_TRY(fence_impl(g));
+  const size_t n = g->grid_elems();
+  if (!present) {
+    std::memset(dst, 0, n * sizeof(double2));
+    return Status::ok();
+  }
+  if (layout == HPGB_LAYOUT_LEFT) {
+    HPGB_CUDA_TRY(cudaMemcpy(dst, buf.ptr, n * sizeof(double2),
+                             cudaMemcpyDeviceToHost));
+    return Status::ok();
+  }
+  DevBuf tmp;
+  HPGB_TRY(tmp.reserve(std::max<size_t>(n, 1) * sizeof(double2)));
+  HPGB_TRY(to_layout(g, buf.as<const double2>(), tmp.as<double2>(), layout,
+                     false, g->grid_size));
+  HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  HPGB_CUDA_TRY(cudaMemcpy(dst, tmp.ptr, n * sizeof(double2),
+                           cudaMemcpyDeviceToHost));
+  return Status::ok();
+}
+
+int hpgb_copy_grid(const hpgb_gridder* cg, void* dst, int layout) {
+  return guarded([&]() -> Status {
+    if (!cg || !dst) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    hpgb_gridder* g = const_cast<hpgb_gridder*>(cg);
+    return copy_values(g, g->grid, true, dst, layout);
+  });
+}
+
+int hpgb_copy_model(const hpgb_gridder* cg, void* dst, int layout) {
+  return guarded([&]() -> Status {
+    if (!cg || !dst) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    hpgb_gridder* g = const_cast<hpgb_gridder*>(cg);
+    return copy_values(g, g->model, g->has_model, dst, layout);
+  });
+}
+
+int hpgb_weights_device_ptr(const hpgb_gridder* g, void** ptr, size_t* span) {
+  return guarded([&]() -> Status {
+    if (!g || !ptr) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    *ptr = g->weights.ptr;
+    if (span) *span = g->weight_elems();
+    return Status::ok();
+  });
+}
+
+int hpgb_grid_device_ptr(const hpgb_gridder* g, void** ptr, size_t* span) {
+  return guarded([&]() -> Status {
+    if (!g || !ptr) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    *ptr = g->grid.ptr;
+    if (span) *span = g->grid_elems();
+    return Status::ok();
+  });
+}
+
+int hpgb_model_device_ptr(const hpgb_gridder* g, void** ptr, size_t* span) {
+  return guarded([&]() -> Status {
+    if (!g || !ptr) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    *ptr = g->has_model ? g->model.ptr : nullptr;
+    if (span) *span = g->has_model ? g->grid_elems() : 0;
+    return Status::ok();
+  });
+}
+
+int hpgb_reset_grid(hpgb_gridder* g) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    HPGB_TRY(fence_impl(g));
+    HPGB_TRY(alloc_grid(g, true));
+    HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    return Status::ok();
+  });
+}
+
+int hpgb_reset_model(hpgb_gridder* g) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    HPGB_TRY(fence_impl(g));
+    g->model.release();
+    g->has_model = false;
+    return Status::ok();
+  });
+}
+
+int hpgb_normalize_by_weights(hpgb_gridder* g, double wfactor) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    return normalize_by_weights(g, wfactor);
+  });
+}
+
+int hpgb_apply_grid_fft(hpgb_gridder* g, double norm, int sign, int in_place) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    return fft(g, g->grid, norm, sign, in_place != 0);
+  });
+}
+
+int hpgb_apply_model_fft(hpgb_gridder* g, double norm, int sign, int in_place) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    if (!g->has_model) return Status::ok();  // src/hpg_runtime.hpp:1369
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    return fft(g, g->model, norm, sign, in_place != 0);
+  });
+}
+
+int hpgb_shift_grid(hpgb_gridder* g, int direction) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    return shift(g, g->grid.as<double2>(), direction);
+  });
+}
+
+int hpgb_shift_model(hpgb_gridder* g, int direction) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    if (!g->has_model) return Status::ok();
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    return shift(g, g->model.as<double2>(), direction);
+  });
+}
+
+int hpgb_kernel_launches(const hpgb_gridder* g, uint64_t* count) {
+  return guarded([&]() -> Status {
+    if (!g || !count) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    *count = g->launches;
+    return Status::ok();
+  });
+}
+
+int hpgb_debug_coords(hpgb_gridder* g, const void* vis, size_t n,
+                      unsigned npol, hpgb_vis_coords* out) {
+  return guarded([&]() -> Status {
+    if (!g || (n > 0 && (!vis || !out)))
+      return Status::err(HPGB_ERROR_OTHER, "null argument");
+    if (npol != g->npol)
+      return Status::err(HPGB_ERROR_INVALID_NUMBER_POLARIZATIONS,
+                         "Number of visibility polarizations does not match "
+                         "Mueller matrix");
+    if (!g->cf.set) return Status::err(HPGB_ERROR_OTHER, "no convolution function set");
+    if (n == 0) return Status::ok();
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    HPGB_TRY(fence_impl(g));
+    const size_t rec = visdata_size(npol);
+    DevBuf dv, dout;
+    HPGB_TRY(dv.reserve(n * rec));
+    HPGB_TRY(dout.reserve(n * sizeof(hpgb_vis_coords)));
+    HPGB_CUDA_TRY(cudaMemcpyAsync(dv.ptr, vis, n * rec, cudaMemcpyHostToDevice,
+                                  g->stream));
+    HPGB_TRY(debug_coords(g, dv.ptr, n, dout.as<hpgb_vis_coords>()));
+    HPGB_CUDA_TRY(cudaMemcpyAsync(out, dout.ptr, n * sizeof(hpgb_vis_coords),
+                                  cudaMemcpyDeviceToHost, g->stream));
+    HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    // an out-of-range index shows as in_grid = 0; clear the status bit
+    HPGB_CUDA_TRY(cudaMemset(g->vb.counters.ptr, 0, sizeof(unsigned)));
+    return Status::ok();
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,119 @@
+// gridder.cuh -- host-side state of one hpgb_gridder (one hpg::GridderState).
+#pragma once
+
+#include <cufft.h>
+
+#include <array>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "common.cuh"
+
+namespace hpgb {
+
+// device buffer owned by the gridder
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  Status reserve(size_t n);   // grows, contents not preserved
+  void release();
+  template <typename T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// the CF region: slices of every group plus their sums
+struct CFRegion {
+  unsigned os = 0;
+  std::vector<std::array<unsigned, 4>> extents;  // per group, as given
+  std::vector<CFGroup> groups;                   // host copy of descriptors
+  DevBuf data;      // all slices of all groups
+  DevBuf wsum;      // all slice sums
+  DevBuf desc;      // device copy of groups
+  int max_taps_x = 0, max_taps_y = 0, max_mueller = 0;
+  bool set = false;
+};
+
+// scratch and staging for one visibility batch
+struct VisBuffers {
+  DevBuf vis;       // VisData<N> records (device copy / returned values)
+  DevBuf gvis;      // float2 [n][N] visibility values scaled for gridding
+  // tiled path: sorted work description
+  DevBuf keys, keys_alt, order, order_alt, sort_tmp, buckets, items, counters;
+  DevBuf prep;      // per-visibility prepared records (sorted order)
+};
+
+struct hpgb_gridder_impl;
+
+}  // namespace hpgb
+
+struct hpgb_gridder {
+  int device = 0;
+  unsigned max_added_tasks = 0;
+  size_t max_batch = 0;
+  unsigned grid_size[4] = {0, 0, 0, 0};
+  double grid_scale[2] = {0, 0};
+  unsigned npol = 0;
+  hpgb::MuellerTables mt;
+  int precision = HPGB_PRECISION_FP64;
+
+  cudaStream_t stream = nullptr;
+
+  hpgb::DevBuf grid;      // double2 [cube][mrow][y][x]
+  hpgb::DevBuf weights;   // double  [cube][mrow]
+  hpgb::DevBuf model;     // double2, empty when no model is set
+  bool has_model = false;
+
+  hpgb::CFRegion cf;
+  hpgb::VisBuffers vb;
+
+  // returned-visibility copy pending until the next fence
+  void* pending_dst = nullptr;
+  size_t pending_bytes = 0;
+  bool pending_on_device = false;
+
+  // cuFFT plans by (nx, ny, batch)
+  std::map<std::tuple<int, int, int>, cufftHandle> fft_plans;
+
+  mutable std::mutex mtx;
+  uint64_t launches = 0;  // kernels launched by this gridder
+
+  size_t grid_elems() const {
+    return size_t(grid_size[0]) * grid_size[1] * grid_size[2] * grid_size[3];
+  }
+  size_t weight_elems() const { return size_t(grid_size[2]) * grid_size[3]; }
+  hpgb::GridGeom geom() const;
+};
+
+namespace hpgb {
+
+// cf_layout.cu
+Status cf_region_bytes(unsigned os, unsigned ngroups, const unsigned* extents,
+                       size_t* data_bytes, size_t* wsum_bytes);
+Status set_cf(hpgb_gridder* g, unsigned os, unsigned ngroups,
+              const unsigned* extents, const void* const* values, int layout,
+              bool on_device);
+Status copy_cf(hpgb_gridder* dst, const hpgb_gridder* src);
+
+// grid_direct.cu
+Status grid_direct(hpgb_gridder* g, const void* d_vis, size_t n,
+                   unsigned flags);
+Status debug_coords(hpgb_gridder* g, const void* d_vis, size_t n,
+                    hpgb_vis_coords* d_out);
+
+// imaging.cu
+Status normalize_by_weights(hpgb_gridder* g, double wfactor);
+Status scale_grid(hpgb_gridder* g, double2* grid, double norm);
+Status shift(hpgb_gridder* g, double2* grid, int direction);
+Status fft(hpgb_gridder* g, DevBuf& grid, double norm, int sign, bool in_place);
+Status to_layout(hpgb_gridder* g, const double2* src, double2* dst,
+                 int layout, bool to_device_layout, const unsigned* ext);
+Status weights_to_layout(hpgb_gridder* g, const double* src, double* dst,
+                         int layout);
+void release_fft_plans(hpgb_gridder* g);
+
+}  // namespace hpgb

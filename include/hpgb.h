@@ -1,0 +1,263 @@
+/*
+ * hpgb.h -- C ABI of libhpgb.so, the sm_100a (B200) gridding / degridding
+ * device for HPG (hannajonathan/hpg v2.0.1).
+ *
+ * The reference selects its device implementation through the abstract class
+ * hpg::runtime::State (src/hpg_runtime.hpp:80-207); StateT<Device::Cuda>
+ * (src/hpg_runtime.hpp:721-1750) is its Kokkos/CUDA implementation.  Every
+ * entry point below replaces one State virtual (or one StateT constructor),
+ * named in its comment, so that a host-side State subclass can forward each
+ * virtual to exactly one call here.  The C++ API in hpg_b200/cpp does that.
+ *
+ * Conventions
+ *  - Every function returns an int status: HPGB_SUCCESS (0) or 1 + the value
+ *    of the matching hpg::ErrorType (src/hpg_error.hpp:26-38).  Failures that
+ *    have no ErrorType (CUDA or cuFFT errors, bad arguments) return
+ *    HPGB_ERROR_OTHER.  hpgb_last_error_message() describes the last failure
+ *    on the calling thread.  No C++ exception crosses this interface.
+ *  - Work is asynchronous on the gridder's CUDA stream, as in the reference
+ *    (one stream per task, src/hpg_runtime.hpp:1496-1588); hpgb_fence() waits
+ *    for it.  Functions that hand data to the host (hpgb_copy_*) fence first.
+ *  - Grid and model values are complex<double> in the device layout of the
+ *    reference's CUDA device, LayoutLeft [x, y, mrow, cube] (x fastest;
+ *    src/hpg_impl.hpp:190-219).  Weights are double, [mrow, cube] LayoutLeft.
+ *  - Visibilities are arrays of hpgb_visdataN, byte-for-byte the layout of
+ *    hpg::VisData<N> (src/hpg.hpp:236-311).
+ */
+#ifndef HPGB_H
+#define HPGB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HPGB_API __attribute__((visibility("default")))
+#else
+#define HPGB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HPGB_ABI_VERSION 1
+
+/* status codes: 1 + hpg::ErrorType (src/hpg_error.hpp:26-38) */
+enum hpgb_status {
+  HPGB_SUCCESS = 0,
+  HPGB_ERROR_DISABLED_DEVICE = 1,
+  HPGB_ERROR_DISABLED_HOST_DEVICE = 2,
+  HPGB_ERROR_OUT_OF_BOUNDS_CF_INDEX = 3,
+  HPGB_ERROR_INVALID_NUMBER_MUELLER_INDEX_ROWS = 4,
+  HPGB_ERROR_INVALID_NUMBER_POLARIZATIONS = 5,
+  HPGB_ERROR_INVALID_CF_LAYOUT = 6,
+  HPGB_ERROR_INVALID_MODEL_GRID_SIZE = 7,
+  HPGB_ERROR_EXCESSIVE_NUMBER_VISIBILITIES = 8,
+  HPGB_ERROR_UPDATE_WEIGHTS_WITHOUT_GRIDDING = 9,
+  HPGB_ERROR_CF_SUPPORT_EXCEEDS_GRID = 10,
+  HPGB_ERROR_OTHER = 11
+};
+
+/* grid_visibilities flags: the four booleans of State::grid_visibilities
+ * (src/hpg_runtime.hpp:147-154) */
+enum hpgb_grid_flags {
+  HPGB_UPDATE_GRID_WEIGHTS = 1u,
+  HPGB_DO_DEGRID = 2u,
+  HPGB_RETURN_VISIBILITIES = 4u,
+  HPGB_DO_GRID = 8u
+};
+
+/* hpg::Layout (src/hpg.hpp:611-614) */
+enum hpgb_layout { HPGB_LAYOUT_RIGHT = 0, HPGB_LAYOUT_LEFT = 1 };
+
+/* hpg::FFTSign (src/hpg.hpp:965-968) */
+enum hpgb_fft_sign { HPGB_FFT_POSITIVE = 0, HPGB_FFT_NEGATIVE = 1 };
+
+/* hpg::ShiftDirection (src/hpg.hpp:989-992) */
+enum hpgb_shift_direction { HPGB_SHIFT_FORWARD = 0, HPGB_SHIFT_BACKWARD = 1 };
+
+/* Arithmetic form of the gridding kernels.
+ *  FP64:  the reference's arithmetic (FP32 CF x visibility products, FP64
+ *         sums, FP64 grid accumulation, FP64 degridding).
+ *  MIXED: FP32 products and FP32 shared-memory tiles, merged into the FP64
+ *         grid by compensated (two-sum) flushes; coordinates, phases and
+ *         weight sums stay FP64. */
+enum hpgb_precision { HPGB_PRECISION_FP64 = 0, HPGB_PRECISION_MIXED = 1 };
+
+/* Layout of CF values handed to hpgb_set_cf (one buffer per CF group).
+ *  LOGICAL: complex<float> indexed like CFArray::operator()(x, y, mueller,
+ *           cube) (src/hpg.hpp:677-684), rightmost index fastest:
+ *           ((x*ext[1] + y)*ext[2] + mueller)*ext[3] + cube.
+ *  CUDA_V0: the reference CUDA device layout "0-Cuda", LayoutLeft
+ *           [x_major, y_major, mueller, cube, x_minor, y_minor]
+ *           (src/hpg_impl.hpp:238-281).
+ *  HOST_V0: the reference host device layout "0-Serial"/"0-OpenMP", strided
+ *           with axis order mueller, y_major, x_major, cube, x_minor, y_minor
+ *           (src/hpg_impl.hpp:229-235). */
+enum hpgb_cf_layout {
+  HPGB_CF_LAYOUT_LOGICAL = 0,
+  HPGB_CF_LAYOUT_CUDA_V0 = 1,
+  HPGB_CF_LAYOUT_HOST_V0 = 2
+};
+
+/* hpg::VisData<N> (src/hpg.hpp:236-311), same member order and padding */
+#define HPGB_VISDATA_FIELDS(N)                                              \
+  float visibilities[N][2]; /* complex<float> values, by polarization */    \
+  float weights[N];                                                         \
+  double frequency;                                                         \
+  double phase;                                                             \
+  double uvw[3];                                                            \
+  unsigned grid_cube;                                                       \
+  unsigned cf_index[2]; /* (cube, group) */                                 \
+  double cf_phase_gradient[2];
+
+typedef struct hpgb_visdata1 { HPGB_VISDATA_FIELDS(1) } hpgb_visdata1;
+typedef struct hpgb_visdata2 { HPGB_VISDATA_FIELDS(2) } hpgb_visdata2;
+typedef struct hpgb_visdata3 { HPGB_VISDATA_FIELDS(3) } hpgb_visdata3;
+typedef struct hpgb_visdata4 { HPGB_VISDATA_FIELDS(4) } hpgb_visdata4;
+
+/* per-visibility coordinates reported by hpgb_debug_coords: the values
+ * computed by compute_vis_coord() and the Vis constructor
+ * (src/hpg_core.hpp:422-446, :513-550) */
+typedef struct hpgb_vis_coords {
+  int32_t grid_coord[2];  /* left edge of the CF support on the grid */
+  int32_t cf_major[2];
+  int32_t cf_minor[2];
+  int32_t fine_offset[2];
+  int32_t cf_size[2];     /* support (taps) */
+  int32_t pos_w;          /* uvw[2] > 0 */
+  int32_t in_grid;        /* all_within_grid() (src/hpg_core.hpp:1070-1080) */
+} hpgb_vis_coords;
+
+typedef struct hpgb_gridder hpgb_gridder;
+
+/* ABI version of the loaded library (HPGB_ABI_VERSION). */
+HPGB_API int hpgb_abi_version(void);
+
+/* Message for the last failure on this thread ("" if none). */
+HPGB_API const char* hpgb_last_error_message(void);
+
+/* Number of usable CUDA devices (hpg::devices(), src/hpg.hpp:133-135). */
+HPGB_API int hpgb_device_count(int* count);
+
+/* StateT<Cuda> constructor (src/hpg_runtime.hpp:757-781) behind
+ * GridderState::create (src/hpg.cc:226-264).  mueller_indexes and
+ * conjugate_mueller_indexes are row-major [grid_size[2]][num_polarizations],
+ * -1 marking an unused element; rows beyond grid_size[2] and columns beyond
+ * num_polarizations are inactive.  The reference's init_cf_shape argument
+ * maps to a following hpgb_allocate_cf_region call.  DisabledDevice when
+ * device_id names no usable device (device_id < 0 selects device 0). */
+HPGB_API int hpgb_create(int device_id, unsigned max_added_tasks,
+                size_t max_visibility_batch_size, const unsigned grid_size[4],
+                const double grid_scale[2], unsigned num_polarizations,
+                const int* mueller_indexes,
+                const int* conjugate_mueller_indexes,
+                hpgb_gridder** gridder);
+
+/* StateT copy constructor (src/hpg_runtime.hpp:783-799): fences the source
+ * and deep-copies grid, weights, model and CF. */
+HPGB_API int hpgb_clone(const hpgb_gridder* src, hpgb_gridder** gridder);
+
+/* ~StateT (src/hpg_runtime.hpp:827-842): fences, then frees everything. */
+HPGB_API int hpgb_destroy(hpgb_gridder* gridder);
+
+/* Select the arithmetic form (enum hpgb_precision) of later gridding calls. */
+HPGB_API int hpgb_set_precision(hpgb_gridder* gridder, int precision);
+
+/* The CUDA stream (cudaStream_t) all work of this gridder is issued on. */
+HPGB_API int hpgb_get_stream(const hpgb_gridder* gridder, void** stream);
+
+/* State::convolution_function_region_size (src/hpg_runtime.hpp:131-133):
+ * device bytes the CF region needs for a CF of this shape. */
+HPGB_API int hpgb_cf_region_size(const hpgb_gridder* gridder, unsigned oversampling,
+                        unsigned num_groups, const unsigned* extents,
+                        size_t* bytes);
+
+/* State::allocate_convolution_function_region (src/hpg_runtime.hpp:135-136). */
+HPGB_API int hpgb_allocate_cf_region(hpgb_gridder* gridder, unsigned oversampling,
+                            unsigned num_groups, const unsigned* extents);
+
+/* State::set_convolution_function (src/hpg_runtime.hpp:138-139, impl
+ * :890-915).  extents: [num_groups][4] (x, y, mueller, cube) in oversampled
+ * units; values[g]: complex<float> buffer of group g in the given
+ * hpgb_cf_layout, in host memory (values_on_device 0) or device memory.
+ * Returns CFSupportExceedsGrid as the reference does. */
+HPGB_API int hpgb_set_cf(hpgb_gridder* gridder, unsigned oversampling,
+                unsigned num_groups, const unsigned* extents,
+                const void* const* values, int layout, int values_on_device);
+
+/* State::set_model (src/hpg_runtime.hpp:141-142, impl :917-963).
+ * values: complex<double> of extents[4] in hpgb_layout order. */
+HPGB_API int hpgb_set_model(hpgb_gridder* gridder, const void* values,
+                   const unsigned extents[4], int layout, int values_on_device);
+
+/* State::grid_visibilities (src/hpg_runtime.hpp:144-151, impl :965-1188).
+ * visibilities: num_visibilities hpgb_visdataN records with N =
+ * num_polarizations, in host memory (vis_on_device 0) or device memory.
+ * flags: hpgb_grid_flags.  When HPGB_RETURN_VISIBILITIES is set, the
+ * predicted or residual records are written to returned (host or device
+ * memory, same kind as the input; may equal visibilities) and are valid after
+ * the next hpgb_fence().  Validation order of the reference
+ * (src/hpg_runtime.hpp:1816-1828): ExcessiveNumberVisibilities,
+ * InvalidNumberPolarizations, UpdateWeightsWithoutGridding. */
+HPGB_API int hpgb_grid_visibilities(hpgb_gridder* gridder, const void* visibilities,
+                           size_t num_visibilities, unsigned num_polarizations,
+                           unsigned flags, int vis_on_device, void* returned);
+
+/* State::fence (src/hpg_runtime.hpp:153-154). */
+HPGB_API int hpgb_fence(const hpgb_gridder* gridder);
+
+/* State::grid_weights (:156-157): copy weights to host dst in layout. */
+HPGB_API int hpgb_copy_weights(const hpgb_gridder* gridder, double* dst, int layout);
+
+/* State::grid_values (:165-166): copy the grid to host dst in layout. */
+HPGB_API int hpgb_copy_grid(const hpgb_gridder* gridder, void* dst, int layout);
+
+/* State::model_values (:174-175): copy the model to host dst in layout;
+ * zeros when no model is set (UnallocatedModelValueArray). */
+HPGB_API int hpgb_copy_model(const hpgb_gridder* gridder, void* dst, int layout);
+
+/* State::grid_weights_ptr/_span, grid_values_ptr/_span,
+ * model_values_ptr/_span (:159-183): device pointers and element counts,
+ * without a fence.  The model pointer is NULL when no model is set. */
+HPGB_API int hpgb_weights_device_ptr(const hpgb_gridder* gridder, void** ptr,
+                            size_t* span);
+HPGB_API int hpgb_grid_device_ptr(const hpgb_gridder* gridder, void** ptr,
+                         size_t* span);
+HPGB_API int hpgb_model_device_ptr(const hpgb_gridder* gridder, void** ptr,
+                          size_t* span);
+
+/* State::reset_grid / reset_model (:171, :186). */
+HPGB_API int hpgb_reset_grid(hpgb_gridder* gridder);
+HPGB_API int hpgb_reset_model(hpgb_gridder* gridder);
+
+/* State::normalize_by_weights (:189, impl :1293-1310). */
+HPGB_API int hpgb_normalize_by_weights(hpgb_gridder* gridder, double wfactor);
+
+/* State::apply_grid_fft / apply_model_fft (:192-196, impl :1312-1426). */
+HPGB_API int hpgb_apply_grid_fft(hpgb_gridder* gridder, double norm, int sign,
+                        int in_place);
+HPGB_API int hpgb_apply_model_fft(hpgb_gridder* gridder, double norm, int sign,
+                         int in_place);
+
+/* State::shift_grid / shift_model (:198-202, impl :1428-1456). */
+HPGB_API int hpgb_shift_grid(hpgb_gridder* gridder, int direction);
+HPGB_API int hpgb_shift_model(hpgb_gridder* gridder, int direction);
+
+/* Number of CUDA kernels this gridder has launched since it was created
+ * (instrumentation for benchmarks; no counterpart in the reference). */
+HPGB_API int hpgb_kernel_launches(const hpgb_gridder* gridder,
+                                  uint64_t* count);
+
+/* Debug: coordinates the device computes for each visibility (host input,
+ * host output), for bit-exact comparison with the reference's
+ * compute_vis_coord().  No counterpart in the reference's State. */
+HPGB_API int hpgb_debug_coords(hpgb_gridder* gridder, const void* visibilities,
+                      size_t num_visibilities, unsigned num_polarizations,
+                      hpgb_vis_coords* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPGB_H */
