@@ -46,6 +46,10 @@ SHIFT_BACKWARD = 1
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 
+KERNEL_AUTO = 0
+KERNEL_DIRECT = 1
+KERNEL_TILED = 2
+
 CF_LAYOUT_LOGICAL = 0
 CF_LAYOUT_CUDA_V0 = 1
 CF_LAYOUT_HOST_V0 = 2
@@ -100,6 +104,7 @@ SIGNATURES = {
     "hpgb_clone": ([_P, _PP], _I),
     "hpgb_destroy": ([_P], _I),
     "hpgb_set_precision": ([_P, _I], _I),
+    "hpgb_set_gridding_kernel": ([_P, _I], _I),
     "hpgb_get_stream": ([_P, _PP], _I),
     "hpgb_cf_region_size": ([_P, _U, _U, _P, ctypes.POINTER(_S)], _I),
     "hpgb_allocate_cf_region": ([_P, _U, _U, _P], _I),

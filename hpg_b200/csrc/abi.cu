@@ -50,14 +50,19 @@ Status check_status_word(hpgb_gridder* g) {
   if (!g->vb.counters.ptr) return Status::ok();
   HPGB_CUDA_TRY(cudaMemcpy(&h, g->vb.counters.ptr, sizeof(unsigned),
                            cudaMemcpyDeviceToHost));
-  if (h & kStatusBadIndex) {
+  if (h != 0) {
     HPGB_CUDA_TRY(cudaMemsetAsync(g->vb.counters.ptr, 0, sizeof(unsigned),
                                   g->stream));
     HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  }
+  if (h & kStatusWaitTimeout)
+    return Status::err(HPGB_ERROR_OTHER,
+                       "a device-side wait gave up after its iteration limit; "
+                       "results of the last batch are incomplete");
+  if (h & kStatusBadIndex)
     return Status::err(HPGB_ERROR_OUT_OF_BOUNDS_CF_INDEX,
                        "visibility cf_index or grid_cube out of bounds; "
                        "the visibility was skipped");
-  }
   return Status::ok();
 }
 
@@ -232,6 +237,7 @@ int hpgb_clone(const hpgb_gridder* src, hpgb_gridder** out) {
     g->npol = src->npol;
     g->mt = src->mt;
     g->precision = src->precision;
+    g->kernel_kind = src->kernel_kind;
     HPGB_CUDA_TRY(cudaSetDevice(g->device));
     HPGB_CUDA_TRY(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
     HPGB_TRY(g->vb.counters.reserve(256));
@@ -276,6 +282,17 @@ int hpgb_set_precision(hpgb_gridder* g, int precision) {
     if (precision != HPGB_PRECISION_FP64 && precision != HPGB_PRECISION_MIXED)
       return Status::err(HPGB_ERROR_OTHER, "unknown precision");
     g->precision = precision;
+    return Status::ok();
+  });
+}
+
+int hpgb_set_gridding_kernel(hpgb_gridder* g, int kind) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    if (kind != HPGB_KERNEL_AUTO && kind != HPGB_KERNEL_DIRECT &&
+        kind != HPGB_KERNEL_TILED)
+      return Status::err(HPGB_ERROR_OTHER, "unknown kernel kind");
+    g->kernel_kind = kind;
     return Status::ok();
   });
 }
@@ -367,6 +384,7 @@ int hpgb_set_model(hpgb_gridder* g, const void* values, const unsigned ext[4],
     }
     HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
     g->has_model = true;
+    g->model32_valid = false;
     return Status::ok();
   });
 }
@@ -519,6 +537,7 @@ int hpgb_reset_model(hpgb_gridder* g) {
     HPGB_TRY(fence_impl(g));
     g->model.release();
     g->has_model = false;
+    g->model32_valid = false;
     return Status::ok();
   });
 }
@@ -544,6 +563,7 @@ int hpgb_apply_model_fft(hpgb_gridder* g, double norm, int sign, int in_place) {
     if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
     if (!g->has_model) return Status::ok();  // src/hpg_runtime.hpp:1369
     HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    g->model32_valid = false;
     return fft(g, g->model, norm, sign, in_place != 0);
   });
 }
@@ -561,6 +581,7 @@ int hpgb_shift_model(hpgb_gridder* g, int direction) {
     if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
     if (!g->has_model) return Status::ok();
     HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    g->model32_valid = false;
     return shift(g, g->model.as<double2>(), direction);
   });
 }

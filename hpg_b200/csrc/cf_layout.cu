@@ -16,7 +16,7 @@ namespace hpgb {
 namespace {
 
 struct GroupShape {
-  int taps_x, taps_y, nmueller, ncube, nfine;
+  int taps_x, taps_y, nmueller, ncube, nfine, plane_stride;
   long long nslices, slice_stride;
 };
 
@@ -33,8 +33,8 @@ GroupShape group_shape(unsigned os, const unsigned* ext) {
   s.ncube = int(ext[3]);
   s.nfine = 2 * int(os / 2) + 1;
   s.nslices = (long long)s.ncube * s.nfine * s.nfine;
-  const long long elems = (long long)s.nmueller * s.taps_x * s.taps_y;
-  s.slice_stride = (elems + 1) & ~1LL;  // 16-byte multiple
+  s.plane_stride = (s.taps_x * s.taps_y + 1) & ~1;  // 16-byte multiple
+  s.slice_stride = (long long)s.nmueller * s.plane_stride;
   return s;
 }
 
@@ -44,7 +44,7 @@ struct LayoutArgs {
   int layout;
   int os, nfine;
   unsigned ext[4];
-  int taps_x, taps_y, nmueller, ncube;
+  int taps_x, taps_y, nmueller, ncube, plane_stride;
   long long slice_stride;
   long long total;  // nslices * nmueller * taps_y * taps_x
 };
@@ -84,21 +84,21 @@ __global__ void cf_layout_kernel(LayoutArgs a) {
       }
       v = a.in[idx];
     }
-    a.out[s * a.slice_stride + r + (long long)m * a.taps_y * a.taps_x] = v;
+    a.out[s * a.slice_stride + (long long)m * a.plane_stride + r] = v;
   }
 }
 
 // one warp per (slice, mueller): FP64 sum of the taps_x*taps_y values
 __global__ void cf_wsum_kernel(const float2* data, double2* wsum,
                                long long nslices, int nmueller, int taps,
-                               long long slice_stride) {
+                               int plane_stride, long long slice_stride) {
   const long long warp =
       (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= nslices * nmueller) return;
   const long long s = warp / nmueller;
   const int m = int(warp - s * nmueller);
-  const float2* p = data + s * slice_stride + (long long)m * taps;
+  const float2* p = data + s * slice_stride + (long long)m * plane_stride;
   double sx = 0, sy = 0;
   for (int i = lane; i < taps; i += 32) {
     const float2 v = p[i];
@@ -215,6 +215,7 @@ Status set_cf(hpgb_gridder* g, unsigned os, unsigned ngroups,
     a.taps_y = s.taps_y;
     a.nmueller = s.nmueller;
     a.ncube = s.ncube;
+    a.plane_stride = s.plane_stride;
     a.slice_stride = s.slice_stride;
     a.total = s.nslices * s.nmueller * s.taps_x * s.taps_y;
     if (a.total > 0) {
@@ -227,7 +228,8 @@ Status set_cf(hpgb_gridder* g, unsigned os, unsigned ngroups,
       const long long warps = s.nslices * s.nmueller;
       const long long wblocks = (warps * 32 + threads - 1) / threads;
       cf_wsum_kernel<<<unsigned(wblocks), threads, 0, g->stream>>>(
-          out, ws, s.nslices, s.nmueller, s.taps_x * s.taps_y, s.slice_stride);
+          out, ws, s.nslices, s.nmueller, s.taps_x * s.taps_y, s.plane_stride,
+          s.slice_stride);
       HPGB_CUDA_TRY(cudaGetLastError());
       ++g->launches;
     }
@@ -242,6 +244,7 @@ Status set_cf(hpgb_gridder* g, unsigned os, unsigned ngroups,
     d.taps_y = s.taps_y;
     d.nmueller = s.nmueller;
     d.ncube = s.ncube;
+    d.plane_stride = s.plane_stride;
     d.slice_stride = s.slice_stride;
     cf.max_taps_x = std::max(cf.max_taps_x, s.taps_x);
     cf.max_taps_y = std::max(cf.max_taps_y, s.taps_y);

@@ -78,8 +78,9 @@ inline size_t visdata_size(unsigned npol) {
 // value = CF(x = (2 + X)*os + fine_offset_x, y = (2 + Y)*os + fine_offset_y),
 // i.e. the reference's (cf_major + X, cf_minor) indexing of
 // src/hpg_core.hpp:623-631 with both cf_major branches folded into the fine
-// offset.  Slices are padded to a multiple of 16 bytes so that each starts
-// 16-byte aligned.  wsum holds, per slice and Mueller element, the FP64 sum
+// offset.  Each Mueller plane is padded to an even number of elements, so
+// every plane and every slice starts 16-byte aligned and is a whole number of
+// 16-byte units (the unit of bulk copies).  wsum holds, per slice and Mueller element, the FP64 sum
 // of the slice's CF values (the visibility-independent part of both the
 // degridding normaliser and the gridding weight).
 
@@ -88,7 +89,8 @@ struct CFGroup {
   const double2* wsum;     // [slice][mueller]
   int taps_x, taps_y;      // 2*radius + 1
   int nmueller, ncube;
-  long long slice_stride;  // float2 elements per slice
+  int plane_stride;        // float2 elements per Mueller plane (even)
+  long long slice_stride;  // float2 elements per slice = nmueller*plane_stride
 };
 
 struct MuellerTables {
@@ -107,7 +109,7 @@ struct GridGeom {
                      // grid_cube is out of range (the visibility is skipped)
 };
 
-enum : unsigned { kStatusBadIndex = 1u };
+enum : unsigned { kStatusBadIndex = 1u, kStatusWaitTimeout = 2u };
 
 // ---------------------------------------------------------------------------
 // exact-rounding arithmetic: every operation rounds once, no FMA contraction,
@@ -225,8 +227,12 @@ __device__ __forceinline__ void vis_coords(const GridGeom& g,
     vc.phi0[d] = __dmul_rn(-grad[d], double(radius * g.os - int(fo)));
     vc.dphi[d] = __dmul_rn(grad[d], double(g.os));
   }
+  // all_within_grid (src/hpg_core.hpp:1070-1080); the fine-offset bound
+  // holds for every finite position and keeps the CF slice index in range
+  // for non-finite ones
   vc.in_grid = 0 <= vc.grid_coord[0] && vc.grid_coord[0] + taps[0] <= g.nx &&
-               0 <= vc.grid_coord[1] && vc.grid_coord[1] + taps[1] <= g.ny;
+               0 <= vc.grid_coord[1] && vc.grid_coord[1] + taps[1] <= g.ny &&
+               abs(vc.fine[0]) <= g.os / 2 && abs(vc.fine[1]) <= g.os / 2;
 }
 
 __device__ __forceinline__ long long slice_index(const GridGeom& g,

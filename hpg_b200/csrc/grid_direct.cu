@@ -89,7 +89,7 @@ degrid_direct_kernel(VisData<N>* vis, size_t n, GridGeom g,
         for (int vpol = 0; vpol < N; ++vpol) {
           const int m = dmi[gpol][vpol];
           if (m >= 0) {
-            float2 cf = slice[m * ncell + c];
+            float2 cf = slice[m * G.plane_stride + c];
             cf.y *= im;
             const double2 p = cmul_d(make_double2(cf.x, cf.y), mv);
             acc[2 * vpol] = __dadd_rn(acc[2 * vpol], p.x);
@@ -186,7 +186,7 @@ grid_direct_kernel(const VisData<N>* vis, size_t n, GridGeom g,
       for (int vpol = 0; vpol < N; ++vpol) {
         const int m = gmi[gpol][vpol];
         if (m >= 0) {
-          float2 cf = slice[m * ncell + c];
+          float2 cf = slice[m * G.plane_stride + c];
           cf.y *= im;
           const float2 p = cmul_f(cmul_f(cf, screen), gv_in[vpol]);
           gx = __dadd_rn(gx, double(p.x));

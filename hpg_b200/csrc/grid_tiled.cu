@@ -1,0 +1,1021 @@
+// grid_tiled.cu -- fused degrid -> residual -> grid over shared-memory uv
+// tiles: the hot path of State::grid_visibilities
+// (src/hpg_runtime.hpp:965-1001 -> VisibilityGridder::kernel,
+// src/hpg_core.hpp:1082-1253), designed for sm_100a.
+//
+// Pipeline of one batch (all on the gridder's stream, no host sync):
+//   1. tile_keys_kernel   coordinates of every visibility (bit-exact with
+//                         compute_vis_coord) -> key = (cube, tile row, tile
+//                         col) of the tile holding the footprint origin;
+//                         histogram of keys
+//   2. cub radix sort     stable sort of (key, visibility index)
+//   3. scans + chunks     tile starts; work chunks of <= kChunkVis visibilities
+//   4. tile_desc_kernel   one 256-byte descriptor per visibility in sorted
+//                         order (tile-relative footprint origin, phasor,
+//                         phase screen, degridding normaliser and grid-row
+//                         weights from the per-slice CF sums, gridding
+//                         values) + the address of its CF slice
+//   5. tiled_kernel       persistent, one thread-block cluster per tile with
+//                         one CTA per grid row (Mueller row) r:
+//                         - a producer warp streams each visibility's
+//                           descriptor and the CF planes row r needs
+//                           (Mueller row r of both index sets) into a ring of
+//                           shared-memory slots with cp.async.bulk, mbarrier
+//                           completion, and prefetches later slices into L2;
+//                         - the model tile of row r is loaded once per chunk
+//                           with a 3-D TMA tensor copy;
+//                         - 8 consumer warps degrid the visibility against
+//                           the model tile (partial sums of row r), exchange
+//                           the partials with the other rows' CTAs through
+//                           distributed shared memory and a remote mbarrier,
+//                           form the prediction and residual (identically in
+//                           every CTA), and grid the scaled residual into the
+//                           row's shared-memory grid tile; the gridding of
+//                           visibility j overlaps the exchange of j+1;
+//                         - at the end of a chunk the tile is added to the
+//                           FP64 grid with red.global.add.f64, and the row's
+//                           weight sum to the weights.
+// Each CF value therefore crosses HBM once per visibility, the model and grid
+// tiles once per chunk.
+//
+// Arithmetic forms:
+//   FP64  (reference arithmetic): FP64 model tile, FP64 degridding products
+//         (FMA), gridding products in FP32 with the reference's rounding
+//         (cf*screen*gvis, no contraction), FP64 sum over polarizations, FP64
+//         shared-memory tile.
+//   MIXED FP32 model tile, FP32 products and per-thread FP32 partial sums
+//         (merged in FP64 across threads, rows and in the normalisation),
+//         FP32 shared-memory tile flushed into the FP64 grid every chunk.
+//         Coordinates, phases, normalisers and weight sums stay FP64.
+
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <cub/cub.cuh>
+#include <type_traits>
+
+#include "gridder.cuh"
+#include "ptx.cuh"
+
+namespace hpgb {
+
+namespace {
+
+constexpr int kConsumerWarps = 8;
+constexpr int kConsumers = kConsumerWarps * 32;
+constexpr int kThreadsTiled = kConsumers + 32;
+constexpr int kMaxSlots = 4;
+constexpr int kChunkVisFP64 = 2048;
+constexpr int kChunkVisMixed = 256;
+constexpr int kMaxRuns = 8;
+
+struct alignas(16) TileDesc {
+  int32_t index;         // visibility index in the batch
+  int16_t cx, cy;        // footprint origin relative to the tile region
+  uint8_t taps_x, taps_y, flags, pad0;
+  int32_t pstride;       // CF plane stride (float2 elements)
+  double2 phasor;        // cphase(phase)
+  double phi0[2], dphi[2];
+  float2 vals[4];
+  float weights[4];
+  double2 den[4];        // degridding normaliser per polarization
+  double twgt[4];        // grid weight increment per grid row
+  float2 gvis[4];        // values scaled for gridding (used without degrid)
+  int32_t pad1[4];
+};
+static_assert(sizeof(TileDesc) == 256, "TileDesc is one 256-byte bulk copy");
+
+enum : uint8_t { kPosW = 1, kScreen = 2 };
+
+struct SliceRef {
+  long long off;  // float2 offset of the slice in the CF region
+  int pstride;
+  int ncell;
+};
+
+struct Chunk {
+  int tile, start, count, pad;
+};
+
+struct TiledParams {
+  int nx, ny, nrow, ncube;
+  int R, T, ntx, nty;
+  int D, slot_bytes, model_bytes;
+  int esize_model, esize_grid;  // bytes per tile element; 0 when unused
+  int nplanes[4];
+  int nruns[4];
+  int run_plane[4][kMaxRuns];
+  int run_len[4][kMaxRuns];
+  int run_dst[4][kMaxRuns];
+  int dpos[4][2][4];  // [row][pos_w][vpol] -> plane position in the slot
+  int gpos[4][2][4];
+  int do_degrid, do_grid, update_weights, has_model;
+  const TileDesc* descs;
+  const SliceRef* srefs;
+  const Chunk* chunks;
+  const unsigned* num_chunks;
+  const float2* cf;
+  double2* grid;
+  double* weights;
+  unsigned char* records;  // VisData<N> records (values written back)
+  int rec_stride;
+  unsigned* status;
+};
+
+struct SmemLayout {
+  int bars, xbuf, wred, bcast, desc, ring, model, grid, total;
+};
+
+__host__ __device__ inline int align_up(int v, int a) { return (v + a - 1) / a * a; }
+
+__host__ __device__ inline SmemLayout smem_layout(int D, int slot_bytes, int R,
+                                                  int esize_model,
+                                                  int esize_grid) {
+  SmemLayout L;
+  L.bars = 0;                       // 16 mbarriers
+  L.xbuf = 128;                     // [2][4 rows][4 pol] complex double
+  L.wred = L.xbuf + 2 * 4 * 4 * 16; // [warps][8] double
+  L.bcast = L.wred + kConsumerWarps * 8 * 8;  // [2][4] float2
+  L.desc = align_up(L.bcast + 2 * 4 * 8, 128);
+  L.ring = align_up(L.desc + kMaxSlots * int(sizeof(TileDesc)), 1024);
+  L.model = align_up(L.ring + D * slot_bytes, 1024);
+  L.grid = align_up(L.model + R * R * esize_model, 128);
+  L.total = L.grid + R * R * esize_grid;
+  return L;
+}
+
+// ---------------------------------------------------------------------------
+// preparation kernels
+
+struct TileGeom {
+  int T, ntx, nty, ntiles;  // ntiles = ncube * nty * ntx (also the invalid key)
+};
+
+template <int N>
+__global__ void tile_keys_kernel(const VisData<N>* vis, size_t n, GridGeom g,
+                                 const CFGroup* groups, TileGeom tg,
+                                 unsigned* keys, unsigned* order,
+                                 unsigned* counts) {
+  const size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const VisData<N>& vd = vis[i];
+  VisCoord vc;
+  vis_coords(g, groups, vd.freq, vd.uvw, vd.grid_cube, vd.cf_index,
+             vd.cf_phase_gradient, vc);
+  unsigned key = unsigned(tg.ntiles);
+  if (vc.in_grid) {
+    key = unsigned((vc.grid_cube * tg.nty + vc.grid_coord[1] / tg.T) * tg.ntx +
+                   vc.grid_coord[0] / tg.T);
+    atomicAdd(&counts[key], 1u);
+  }
+  keys[i] = key;
+  order[i] = unsigned(i);
+}
+
+__global__ void chunk_count_kernel(const unsigned* counts, int ntiles, int K,
+                                   unsigned* nch) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < ntiles) nch[t] = (counts[t] + K - 1) / K;
+}
+
+__global__ void chunk_write_kernel(const unsigned* counts,
+                                   const unsigned* tstart,
+                                   const unsigned* nch, const unsigned* cstart,
+                                   int ntiles, int K, Chunk* chunks,
+                                   unsigned* num_chunks) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  for (unsigned k = 0; k < nch[t]; ++k) {
+    Chunk c;
+    c.tile = t;
+    c.start = int(tstart[t] + k * K);
+    c.count = int(min(unsigned(K), counts[t] - k * K));
+    c.pad = 0;
+    chunks[cstart[t] + k] = c;
+  }
+  if (t == ntiles - 1) *num_chunks = cstart[t] + nch[t];
+}
+
+template <int N>
+__global__ void tile_desc_kernel(const VisData<N>* vis, const unsigned* order,
+                                 const unsigned* keys, size_t n, GridGeom g,
+                                 const CFGroup* groups, TileGeom tg,
+                                 const float2* cf_base, TileDesc* descs,
+                                 SliceRef* srefs) {
+  const size_t pidx = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+  if (pidx >= n) return;
+  const unsigned key = keys[pidx];
+  if (key >= unsigned(tg.ntiles)) return;
+  const unsigned i = order[pidx];
+  const VisData<N>& vd = vis[i];
+  VisCoord vc;
+  vis_coords(g, groups, vd.freq, vd.uvw, vd.grid_cube, vd.cf_index,
+             vd.cf_phase_gradient, vc);
+  const CFGroup& G = groups[vc.grp];
+  const int tx = int(key % unsigned(tg.ntx));
+  const int ty = int((key / unsigned(tg.ntx)) % unsigned(tg.nty));
+  TileDesc d;
+  d.index = int(i);
+  d.cx = int16_t(vc.grid_coord[0] - tx * tg.T);
+  d.cy = int16_t(vc.grid_coord[1] - ty * tg.T);
+  d.taps_x = uint8_t(vc.taps[0]);
+  d.taps_y = uint8_t(vc.taps[1]);
+  const bool screen_on = vc.phi0[0] != 0.0 || vc.phi0[1] != 0.0 ||
+                         vc.dphi[0] != 0.0 || vc.dphi[1] != 0.0;
+  d.flags = (vc.pos_w ? kPosW : 0) | (screen_on ? kScreen : 0);
+  d.pad0 = 0;
+  d.pstride = G.plane_stride;
+  d.phasor = cphase_d(vd.phase);
+  for (int k = 0; k < 2; ++k) {
+    d.phi0[k] = vc.phi0[k];
+    d.dphi[k] = vc.dphi[k];
+  }
+  const long long sidx = slice_index(g, vc);
+  const double2* ws = G.wsum + sidx * G.nmueller;
+  const int(*dmi)[4] = vc.pos_w ? g.mt.c : g.mt.m;
+  const int(*gmi)[4] = vc.pos_w ? g.mt.m : g.mt.c;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    d.vals[v] = v < N ? vd.vis[v] : make_float2(0.f, 0.f);
+    d.weights[v] = v < N ? vd.weights[v] : 0.f;
+    d.gvis[v] = v < N ? scale_for_gridding(vd.vis[v], d.phasor, vd.weights[v])
+                      : make_float2(0.f, 0.f);
+    // normaliser: sum over grid rows of the slice sums, conjugated for
+    // non-positive w (src/hpg_core.hpp:598-600, :659-661)
+    double2 den = make_double2(0.0, 0.0);
+    if (v < N)
+      for (int r = 0; r < g.nrow; ++r) {
+        const int m = dmi[r][v];
+        if (m >= 0) {
+          const double2 w = ws[m];
+          den = cadd_d(den, make_double2(w.x, vc.pos_w ? w.y : -w.y));
+        }
+      }
+    d.den[v] = den;
+  }
+  // grid weight per row: sum_vpol |sum_XY cf| * w (src/hpg_core.hpp:877-885)
+  for (int r = 0; r < 4; ++r) {
+    double tw = 0.0;
+    if (r < g.nrow)
+      for (int v = 0; v < N; ++v) {
+        const int m = gmi[r][v];
+        if (m >= 0) {
+          const double2 w = ws[m];
+          tw = __dadd_rn(tw, __dmul_rn(hypot(w.x, w.y), double(vd.weights[v])));
+        }
+      }
+    d.twgt[r] = tw;
+  }
+  for (int k = 0; k < 4; ++k) d.pad1[k] = 0;
+  descs[pidx] = d;
+  SliceRef s;
+  s.off = (G.data - cf_base) + sidx * G.slice_stride;
+  s.pstride = G.plane_stride;
+  s.ncell = vc.taps[0] * vc.taps[1];
+  srefs[pidx] = s;
+}
+
+__global__ void model_to_f32_kernel(const double2* __restrict__ in,
+                                    float2* __restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const double2 v = in[i];
+    out[i] = make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the tiled kernel
+
+template <bool MIXED>
+struct Form;
+
+template <>
+struct Form<false> {
+  using model_t = double2;
+  using grid_t = double2;
+};
+
+template <>
+struct Form<true> {
+  using model_t = float2;
+  using grid_t = float2;
+};
+
+template <int N, bool MIXED>
+__device__ __forceinline__ void degrid_cells(const TiledParams& p,
+                                             const TileDesc& d,
+                                             const float2* cfs, int row,
+                                             const typename Form<MIXED>::model_t* mtile,
+                                             int ctid, double (&acc)[2 * N]) {
+  const bool pos_w = d.flags & kPosW;
+  const bool screen_on = d.flags & kScreen;
+  const int tx = d.taps_x, ncell = int(d.taps_x) * d.taps_y;
+  const float im = pos_w ? 1.0f : -1.0f;
+  int pp[N];
+#pragma unroll
+  for (int v = 0; v < N; ++v) pp[v] = p.dpos[row][pos_w ? 1 : 0][v];
+  if constexpr (!MIXED) {
+    for (int c = ctid; c < ncell; c += kConsumers) {
+      const int Y = c / tx, X = c - Y * tx;
+      double2 mv = mtile[(d.cy + Y) * p.R + d.cx + X];
+      if (screen_on) {
+        const double phx = __dadd_rn(d.phi0[0], __dmul_rn(double(X), d.dphi[0]));
+        const double phy = __dadd_rn(d.phi0[1], __dmul_rn(double(Y), d.dphi[1]));
+        mv = cmul_d(mv, cphase_d(__dsub_rn(-phx, phy)));
+      }
+#pragma unroll
+      for (int v = 0; v < N; ++v) {
+        if (pp[v] >= 0) {
+          const float2 cf = cfs[pp[v] * d.pstride + c];
+          const double cr = cf.x, ci = double(cf.y) * im;
+          acc[2 * v] = fma(cr, mv.x, fma(-ci, mv.y, acc[2 * v]));
+          acc[2 * v + 1] = fma(cr, mv.y, fma(ci, mv.x, acc[2 * v + 1]));
+        }
+      }
+    }
+  } else {
+    float a[2 * N];
+#pragma unroll
+    for (int k = 0; k < 2 * N; ++k) a[k] = 0.f;
+    for (int c = ctid; c < ncell; c += kConsumers) {
+      const int Y = c / tx, X = c - Y * tx;
+      float2 mv = mtile[(d.cy + Y) * p.R + d.cx + X];
+      if (screen_on) {
+        const double phx = __dadd_rn(d.phi0[0], __dmul_rn(double(X), d.dphi[0]));
+        const double phy = __dadd_rn(d.phi0[1], __dmul_rn(double(Y), d.dphi[1]));
+        const double2 s = cphase_d(__dsub_rn(-phx, phy));
+        const float sx = float(s.x), sy = float(s.y);
+        mv = make_float2(mv.x * sx - mv.y * sy, mv.x * sy + mv.y * sx);
+      }
+#pragma unroll
+      for (int v = 0; v < N; ++v) {
+        if (pp[v] >= 0) {
+          const float2 cf = cfs[pp[v] * d.pstride + c];
+          const float ci = cf.y * im;
+          a[2 * v] = fmaf(cf.x, mv.x, fmaf(-ci, mv.y, a[2 * v]));
+          a[2 * v + 1] = fmaf(cf.x, mv.y, fmaf(ci, mv.x, a[2 * v + 1]));
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 2 * N; ++k) acc[k] = a[k];
+  }
+}
+
+template <int N, bool MIXED>
+__device__ __forceinline__ void grid_cells(const TiledParams& p,
+                                           const TileDesc& d, const float2* cfs,
+                                           int row, const float2* gvis,
+                                           typename Form<MIXED>::grid_t* gtile,
+                                           int ctid) {
+  const bool pos_w = d.flags & kPosW;
+  const bool screen_on = d.flags & kScreen;
+  const int tx = d.taps_x, ncell = int(d.taps_x) * d.taps_y;
+  const float im = pos_w ? -1.0f : 1.0f;
+  int pp[N];
+  float2 gv[N];
+#pragma unroll
+  for (int v = 0; v < N; ++v) {
+    pp[v] = p.gpos[row][pos_w ? 1 : 0][v];
+    gv[v] = gvis[v];
+  }
+  for (int c = ctid; c < ncell; c += kConsumers) {
+    const int Y = c / tx, X = c - Y * tx;
+    float2 screen = make_float2(1.0f, 0.0f);
+    if (screen_on) {
+      const double phx = __dadd_rn(d.phi0[0], __dmul_rn(double(X), d.dphi[0]));
+      const double phy = __dadd_rn(d.phi0[1], __dmul_rn(double(Y), d.dphi[1]));
+      const double2 s = cphase_d(__dadd_rn(phx, phy));
+      screen = make_float2(__double2float_rn(s.x), __double2float_rn(s.y));
+    }
+    const int idx = (d.cy + Y) * p.R + d.cx + X;
+    if constexpr (!MIXED) {
+      double sx = 0.0, sy = 0.0;
+#pragma unroll
+      for (int v = 0; v < N; ++v) {
+        if (pp[v] >= 0) {
+          float2 cf = cfs[pp[v] * d.pstride + c];
+          cf.y *= im;
+          const float2 prod =
+              screen_on ? cmul_f(cmul_f(cf, screen), gv[v]) : cmul_f(cf, gv[v]);
+          sx = __dadd_rn(sx, double(prod.x));
+          sy = __dadd_rn(sy, double(prod.y));
+        }
+      }
+      double2 t = gtile[idx];
+      t.x += sx;
+      t.y += sy;
+      gtile[idx] = t;
+    } else {
+      float sx = 0.f, sy = 0.f;
+#pragma unroll
+      for (int v = 0; v < N; ++v) {
+        if (pp[v] >= 0) {
+          float2 cf = cfs[pp[v] * d.pstride + c];
+          cf.y *= im;
+          if (screen_on)
+            cf = make_float2(cf.x * screen.x - cf.y * screen.y,
+                             cf.x * screen.y + cf.y * screen.x);
+          sx = fmaf(cf.x, gv[v].x, fmaf(-cf.y, gv[v].y, sx));
+          sy = fmaf(cf.x, gv[v].y, fmaf(cf.y, gv[v].x, sy));
+        }
+      }
+      float2 t = gtile[idx];
+      t.x += sx;
+      t.y += sy;
+      gtile[idx] = t;
+    }
+  }
+}
+
+template <int N, bool MIXED>
+__global__ void __launch_bounds__(kThreadsTiled, 1)
+tiled_kernel(const __grid_constant__ TiledParams p,
+             const __grid_constant__ CUtensorMap model_map) {
+  using MT = typename Form<MIXED>::model_t;
+  using GT = typename Form<MIXED>::grid_t;
+  extern __shared__ __align__(1024) unsigned char sm_raw[];
+  // TMA destinations want 1024-byte alignment; the launch adds 1 KB of slack
+  unsigned char* sm =
+      sm_raw + ((1024u - (ptx::smem(sm_raw) & 1023u)) & 1023u);
+  // same layout the host sized the launch with (tiles absent when unused)
+  const SmemLayout L =
+      smem_layout(p.D, p.slot_bytes, p.R, p.esize_model, p.esize_grid);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + L.bars);
+  uint64_t* empty = full + kMaxSlots;
+  uint64_t* model_bar = full + 2 * kMaxSlots;
+  uint64_t* xchg = model_bar + 1;
+  double* xbuf = reinterpret_cast<double*>(sm + L.xbuf);  // [2][4][4][2]
+  double* wred = reinterpret_cast<double*>(sm + L.wred);  // [warps][8]
+  float2* bcast = reinterpret_cast<float2*>(sm + L.bcast);  // [2][4]
+  TileDesc* descs = reinterpret_cast<TileDesc*>(sm + L.desc);
+  unsigned char* ring = sm + L.ring;
+  MT* mtile = reinterpret_cast<MT*>(sm + L.model);
+  GT* gtile = reinterpret_cast<GT*>(sm + L.grid);
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int row = int(ptx::cluster_rank());
+  const unsigned cid = ptx::cluster_id_x(), ncl = ptx::num_clusters_x();
+
+  if (tid == 0) {
+    for (int s = 0; s < p.D; ++s) {
+      ptx::mbar_init(&full[s], 1);
+      ptx::mbar_init(&empty[s], kConsumerWarps);
+    }
+    ptx::mbar_init(model_bar, 1);
+    ptx::mbar_init(&xchg[0], uint32_t(p.nrow));
+    ptx::mbar_init(&xchg[1], uint32_t(p.nrow));
+    ptx::fence_mbar_init();
+  }
+  __syncthreads();
+  ptx::cluster_sync();  // every CTA's barriers exist before remote arrivals
+
+  const unsigned nchunks = *p.num_chunks;
+  bool ok = true;
+  const bool exchange = p.do_degrid && p.has_model;
+
+  if (warp == kConsumerWarps) {
+    // ---------------- producer ----------------
+    if (lane == 0) {
+      uint32_t q = 0;
+      for (unsigned c = cid; c < nchunks; c += ncl) {
+        const Chunk ch = p.chunks[c];
+        for (int k = 0; k < ch.count; ++k, ++q) {
+          const int s = int(q % uint32_t(p.D));
+          if (q >= uint32_t(p.D))
+            ok &= ptx::mbar_wait(&empty[s], ((q / p.D) & 1) ^ 1);
+          const int j = ch.start + k;
+          const SliceRef sr = p.srefs[j];
+          const uint32_t pbytes = uint32_t(sr.pstride) * 8u;
+          const uint32_t bytes =
+              uint32_t(sizeof(TileDesc)) + uint32_t(p.nplanes[row]) * pbytes;
+          ptx::mbar_expect_tx(&full[s], bytes);
+          ptx::bulk_g2s(&descs[s], &p.descs[j], uint32_t(sizeof(TileDesc)),
+                        &full[s]);
+          unsigned char* dst = ring + size_t(s) * p.slot_bytes;
+          const float2* slice = p.cf + sr.off;
+          for (int u = 0; u < p.nruns[row]; ++u)
+            ptx::bulk_g2s(dst + p.run_dst[row][u] * pbytes,
+                          slice + size_t(p.run_plane[row][u]) * sr.pstride,
+                          uint32_t(p.run_len[row][u]) * pbytes, &full[s]);
+          // pull the slice of a later visibility of this chunk into L2
+          const int kp = k + p.D + 2;
+          if (kp < ch.count) {
+            const SliceRef sp = p.srefs[ch.start + kp];
+            const uint32_t pb = uint32_t(sp.pstride) * 8u;
+            const float2* sl = p.cf + sp.off;
+            for (int u = 0; u < p.nruns[row]; ++u)
+              ptx::bulk_prefetch_l2(sl + size_t(p.run_plane[row][u]) * sp.pstride,
+                                    uint32_t(p.run_len[row][u]) * pb);
+          }
+        }
+      }
+    }
+  } else {
+    // ---------------- consumers ----------------
+    const int ctid = tid;
+    uint32_t q = 0;
+    uint32_t model_phase = 0;
+    const int RR = p.R * p.R;
+    for (unsigned c = cid; c < nchunks; c += ncl) {
+      const Chunk ch = p.chunks[c];
+      const int tile = ch.tile;
+      const int tx = tile % p.ntx;
+      const int ty = (tile / p.ntx) % p.nty;
+      const int cube = tile / (p.ntx * p.nty);
+      const int x0 = tx * p.T, y0 = ty * p.T;
+      ptx::named_sync(1, kConsumers);
+      if (exchange && ctid == 0) {
+        // earlier generic-proxy reads of the tile precede this async write
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        ptx::mbar_expect_tx(model_bar, uint32_t(p.model_bytes));
+        ptx::tma_load_3d(mtile, &model_map, 2 * x0, y0, cube * p.nrow + row,
+                         model_bar);
+      }
+      if (p.do_grid)
+        for (int i = ctid; i < RR; i += kConsumers) {
+          GT z;
+          z.x = 0;
+          z.y = 0;
+          gtile[i] = z;
+        }
+      if (exchange) {
+        ok &= ptx::mbar_wait(model_bar, model_phase);
+        model_phase ^= 1;
+      }
+      ptx::named_sync(1, kConsumers);
+      double wchunk = 0.0;
+      int prev_s = -1;
+      for (int k = 0; k < ch.count; ++k, ++q) {
+        const int s = int(q % uint32_t(p.D));
+        ok &= ptx::mbar_wait(&full[s], (q / p.D) & 1);
+        const TileDesc& d = descs[s];
+        const float2* cfs =
+            reinterpret_cast<const float2*>(ring + size_t(s) * p.slot_bytes);
+        const int xs = int(q & 1);
+        if (exchange) {
+          double acc[2 * N];
+#pragma unroll
+          for (int t = 0; t < 2 * N; ++t) acc[t] = 0.0;
+          degrid_cells<N, MIXED>(p, d, cfs, row, mtile, ctid, acc);
+#pragma unroll
+          for (int t = 0; t < 2 * N; ++t) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+              acc[t] += __shfl_down_sync(0xffffffffu, acc[t], o);
+          }
+          if (lane == 0) {
+#pragma unroll
+            for (int t = 0; t < 2 * N; ++t) wred[warp * 8 + t] = acc[t];
+          }
+          ptx::named_sync(2, kConsumers);
+          if (ctid == 0) {
+            double tot[2 * N];
+#pragma unroll
+            for (int t = 0; t < 2 * N; ++t) {
+              double sum = wred[t];
+              for (int w = 1; w < kConsumerWarps; ++w) sum += wred[w * 8 + t];
+              tot[t] = sum;
+            }
+            // partials of row `row` into every CTA of the cluster
+            for (int r = 0; r < p.nrow; ++r) {
+#pragma unroll
+              for (int t = 0; t < 2 * N; ++t)
+                ptx::st_cluster_f64(&xbuf[((xs * 4 + row) * 4) * 2 + t],
+                                    uint32_t(r), tot[t]);
+            }
+            for (int r = 0; r < p.nrow; ++r)
+              ptx::mbar_arrive_remote(&xchg[xs], uint32_t(r));
+          }
+        }
+        // grid the previous visibility while the exchange completes
+        if (prev_s >= 0) {
+          if (p.do_grid)
+            grid_cells<N, MIXED>(p, descs[prev_s],
+                                 reinterpret_cast<const float2*>(
+                                     ring + size_t(prev_s) * p.slot_bytes),
+                                 row, &bcast[(xs ^ 1) * 4], gtile, ctid);
+          __syncwarp();
+          if (lane == 0) ptx::mbar_arrive(&empty[prev_s]);
+        }
+        if (ctid == 0) {
+          float2 gout[4];
+          if (p.do_degrid) {
+            float2 pred[4];
+            if (exchange) {
+              ok &= ptx::mbar_wait_cluster(&xchg[xs], (q >> 1) & 1);
+              const double2 cph = make_double2(d.phasor.x, -d.phasor.y);
+#pragma unroll
+              for (int v = 0; v < N; ++v) {
+                double2 num = make_double2(0.0, 0.0);
+                for (int r = 0; r < p.nrow; ++r) {
+                  const double* x = &xbuf[((xs * 4 + r) * 4) * 2];
+                  num.x += x[2 * v];
+                  num.y += x[2 * v + 1];
+                }
+                double2 den = d.den[v];
+                if (den.x == 0.0 && den.y == 0.0) den = make_double2(1.0, 0.0);
+                const double2 qv = cmul_d(cdiv_d(num, den), cph);
+                pred[v] = make_float2(__double2float_rn(qv.x),
+                                      __double2float_rn(qv.y));
+              }
+            } else {
+#pragma unroll
+              for (int v = 0; v < N; ++v) pred[v] = make_float2(0.f, 0.f);
+            }
+            float2* out = reinterpret_cast<float2*>(
+                p.records + size_t(d.index) * p.rec_stride);
+#pragma unroll
+            for (int v = 0; v < N; ++v) {
+              if (p.do_grid) {
+                const float2 r = make_float2(__fsub_rn(d.vals[v].x, pred[v].x),
+                                             __fsub_rn(d.vals[v].y, pred[v].y));
+                if (row == 0) out[v] = r;
+                gout[v] = scale_for_gridding(r, d.phasor, d.weights[v]);
+              } else {
+                if (row == 0) out[v] = pred[v];
+              }
+            }
+          } else {
+#pragma unroll
+            for (int v = 0; v < N; ++v) gout[v] = d.gvis[v];
+          }
+          if (p.do_grid) {
+#pragma unroll
+            for (int v = 0; v < N; ++v) bcast[xs * 4 + v] = gout[v];
+            wchunk += d.twgt[row];
+          }
+        }
+        ptx::named_sync(1, kConsumers);
+        prev_s = s;
+      }
+      if (prev_s >= 0) {
+        if (p.do_grid)
+          grid_cells<N, MIXED>(p, descs[prev_s],
+                               reinterpret_cast<const float2*>(
+                                   ring + size_t(prev_s) * p.slot_bytes),
+                               row, &bcast[((q - 1) & 1) * 4], gtile, ctid);
+        __syncwarp();
+        if (lane == 0) ptx::mbar_arrive(&empty[prev_s]);
+      }
+      ptx::named_sync(1, kConsumers);
+      if (p.do_grid) {
+        double2* plane = p.grid + size_t(cube * p.nrow + row) * p.ny * p.nx;
+        for (int i = ctid; i < RR; i += kConsumers) {
+          const int gx = x0 + i % p.R, gy = y0 + i / p.R;
+          if (gx < p.nx && gy < p.ny) {
+            const GT v = gtile[i];
+            if (v.x != 0 || v.y != 0) {
+              double2* dst = plane + size_t(gy) * p.nx + gx;
+              atomicAdd(&dst->x, double(v.x));
+              atomicAdd(&dst->y, double(v.y));
+            }
+          }
+        }
+        if (ctid == 0 && p.update_weights && ch.count > 0)
+          atomicAdd(p.weights + size_t(cube) * p.nrow + row, wchunk);
+      }
+    }
+  }
+  if (!ok) atomicOr(p.status, kStatusWaitTimeout);
+  __syncwarp();
+  ptx::cluster_sync();  // no CTA leaves while peers may still address it
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault,
+                                &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+struct Plan {
+  bool ok = false;
+  std::string why;
+  int R = 0, T = 0, D = 0, slot_bytes = 0, K = 0;
+  TiledParams p{};
+  int smem = 0;
+};
+
+Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed) {
+  Plan pl;
+  const CFRegion& cf = g->cf;
+  const int nrow = int(g->grid_size[2]);
+  if (cf.groups.empty()) {
+    pl.why = "no CF groups";
+    return pl;
+  }
+  if (nrow < 1 || nrow > 4) {
+    pl.why = "rows";
+    return pl;
+  }
+  TiledParams& p = pl.p;
+  std::memset(&p, 0, sizeof(p));
+  for (int r = 0; r < 4; ++r)
+    for (int v = 0; v < 4; ++v)
+      if (g->mt.m[r][v] >= 64 || g->mt.c[r][v] >= 64) {
+        pl.why = "Mueller index beyond 63";
+        return pl;
+      }
+  // planes each row's CTA needs: Mueller row r of both index sets
+  int max_planes = 0;
+  for (int r = 0; r < nrow; ++r) {
+    bool need[64] = {false};
+    for (int v = 0; v < 4; ++v) {
+      if (g->mt.m[r][v] >= 0) need[g->mt.m[r][v]] = true;
+      if (g->mt.c[r][v] >= 0) need[g->mt.c[r][v]] = true;
+    }
+    int pos[64];
+    int np = 0, nr = 0;
+    for (int m = 0; m < 64; ++m) {
+      pos[m] = -1;
+      if (!need[m]) continue;
+      pos[m] = np;
+      if (m > 0 && need[m - 1]) {
+        p.run_len[r][nr - 1]++;
+      } else {
+        if (nr == kMaxRuns) {
+          pl.why = "too many plane runs";
+          return pl;
+        }
+        p.run_plane[r][nr] = m;
+        p.run_len[r][nr] = 1;
+        p.run_dst[r][nr] = np;
+        ++nr;
+      }
+      ++np;
+    }
+    p.nplanes[r] = np;
+    p.nruns[r] = nr;
+    max_planes = std::max(max_planes, np);
+    for (int w = 0; w < 2; ++w)
+      for (int v = 0; v < 4; ++v) {
+        // pos_w (w = 1): degrid uses conjugate indexes, grid uses indexes
+        const int dm = w ? g->mt.c[r][v] : g->mt.m[r][v];
+        const int gm = w ? g->mt.m[r][v] : g->mt.c[r][v];
+        p.dpos[r][w][v] = dm >= 0 ? pos[dm] : -1;
+        p.gpos[r][w][v] = gm >= 0 ? pos[gm] : -1;
+      }
+  }
+  int max_plane_bytes = 0;
+  for (const CFGroup& G : cf.groups)
+    max_plane_bytes = std::max(max_plane_bytes, G.plane_stride * 8);
+  const int part = align_up(std::max(max_planes * max_plane_bytes, 16), 128);
+  const int esize = mixed ? 8 : 16;
+  const bool do_degrid = flags & HPGB_DO_DEGRID;
+  const bool do_grid = flags & HPGB_DO_GRID;
+  const int em = (do_degrid && g->has_model) ? esize : 0;
+  const int eg = do_grid ? esize : 0;
+  const int budget = 227 * 1024;
+  const int taps = std::max(cf.max_taps_x, cf.max_taps_y);
+  for (int D = kMaxSlots; D >= 2; --D) {
+    const SmemLayout L0 = smem_layout(D, part, 0, em, eg);
+    const int left = budget - L0.total - 1024 - 1024;
+    if (left <= 0) continue;
+    int R = (em + eg) > 0 ? int(std::sqrt(double(left) / double(em + eg))) : 128;
+    R = std::min(R, 128) & ~1;
+    if (R - taps + 1 < 4) continue;
+    pl.D = D;
+    pl.R = R;
+    break;
+  }
+  if (pl.D == 0) {
+    pl.why = "CF slice part too large for the shared-memory ring";
+    return pl;
+  }
+  pl.slot_bytes = part;
+  pl.T = pl.R - taps + 1;
+  pl.K = mixed ? kChunkVisMixed : kChunkVisFP64;
+  pl.smem = smem_layout(pl.D, part, pl.R, em, eg).total + 1024;
+  if (em > 0 && (2 * size_t(g->grid_size[0]) * (mixed ? 4 : 8)) % 16 != 0) {
+    pl.why = "model row pitch not a 16-byte multiple";
+    return pl;
+  }
+  p.nx = int(g->grid_size[0]);
+  p.ny = int(g->grid_size[1]);
+  p.nrow = nrow;
+  p.ncube = int(g->grid_size[3]);
+  p.R = pl.R;
+  p.T = pl.T;
+  p.ntx = (p.nx + pl.T - 1) / pl.T;
+  p.nty = (p.ny + pl.T - 1) / pl.T;
+  p.D = pl.D;
+  p.slot_bytes = part;
+  p.model_bytes = pl.R * pl.R * esize;
+  p.esize_model = em;
+  p.esize_grid = eg;
+  p.do_degrid = do_degrid;
+  p.do_grid = do_grid;
+  p.update_weights = (flags & HPGB_UPDATE_GRID_WEIGHTS) != 0;
+  p.has_model = g->has_model;
+  pl.ok = true;
+  return pl;
+}
+
+template <int N, bool MIXED>
+Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
+                    const CUtensorMap& map) {
+  using MT = typename Form<MIXED>::model_t;
+  using GT = typename Form<MIXED>::grid_t;
+  // the kernel places its tiles with these sizes; they must match the form
+  if ((p.esize_model != 0 && p.esize_model != int(sizeof(MT))) ||
+      (p.esize_grid != 0 && p.esize_grid != int(sizeof(GT))) ||
+      smem_layout(p.D, p.slot_bytes, p.R, p.esize_model, p.esize_grid).total +
+              1024 > smem)
+    return Status::err(HPGB_ERROR_OTHER, "tiled kernel layout mismatch");
+  if ((p.do_degrid && p.has_model && p.esize_model == 0) ||
+      (p.do_grid && p.esize_grid == 0))
+    return Status::err(HPGB_ERROR_OTHER, "tiled kernel tile missing");
+  auto kern = tiled_kernel<N, MIXED>;
+  HPGB_CUDA_TRY(cudaFuncSetAttribute(
+      kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = unsigned(p.nrow);
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cfg.blockDim = dim3(kThreadsTiled);
+  cfg.dynamicSmemBytes = size_t(smem);
+  cfg.stream = g->stream;
+  int sms = 0;
+  HPGB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount,
+                                       g->device));
+  cfg.gridDim = dim3(unsigned(sms / p.nrow * p.nrow));
+  int max_clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&max_clusters, kern, &cfg) == cudaSuccess &&
+      max_clusters > 0)
+    cfg.gridDim = dim3(unsigned(max_clusters * p.nrow));
+  else
+    cudaGetLastError();
+  HPGB_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, p, map));
+  ++g->launches;
+  return Status::ok();
+}
+
+template <int N>
+Status grid_tiled_n(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
+                    const Plan& plan, bool mixed) {
+  VisBuffers& vb = g->vb;
+  const GridGeom geom = g->geom();
+  const CFGroup* groups = g->cf.desc.as<const CFGroup>();
+  TileGeom tg;
+  tg.T = plan.T;
+  tg.ntx = plan.p.ntx;
+  tg.nty = plan.p.nty;
+  tg.ntiles = tg.ntx * tg.nty * int(g->grid_size[3]);
+  const int ntiles = tg.ntiles;
+  const int K = plan.K;
+  const size_t max_chunks = n / K + size_t(ntiles) + 1;
+  // scratch
+  HPGB_TRY(vb.keys.reserve(n * 4));
+  HPGB_TRY(vb.keys_alt.reserve(n * 4));
+  HPGB_TRY(vb.order.reserve(n * 4));
+  HPGB_TRY(vb.order_alt.reserve(n * 4));
+  HPGB_TRY(vb.buckets.reserve(size_t(ntiles + 1) * 4 * 4));
+  HPGB_TRY(vb.items.reserve(max_chunks * sizeof(Chunk)));
+  HPGB_TRY(vb.prep.reserve(n * (sizeof(TileDesc) + sizeof(SliceRef))));
+  unsigned* counts = vb.buckets.as<unsigned>();
+  unsigned* tstart = counts + (ntiles + 1);
+  unsigned* nch = tstart + (ntiles + 1);
+  unsigned* cstart = nch + (ntiles + 1);
+  unsigned* num_chunks = vb.counters.as<unsigned>() + 1;
+  TileDesc* descs = vb.prep.as<TileDesc>();
+  SliceRef* srefs = reinterpret_cast<SliceRef*>(vb.prep.as<char>() +
+                                                n * sizeof(TileDesc));
+  // CUB scratch sizing
+  int end_bit = 1;
+  while ((1ll << end_bit) <= (long long)ntiles) ++end_bit;
+  size_t sort_bytes = 0, scan_bytes = 0;
+  cub::DoubleBuffer<unsigned> kbuf(vb.keys.as<unsigned>(), vb.keys_alt.as<unsigned>());
+  cub::DoubleBuffer<unsigned> vbuf(vb.order.as<unsigned>(), vb.order_alt.as<unsigned>());
+  HPGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, kbuf, vbuf,
+                                                int(n), 0, end_bit, g->stream));
+  HPGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts,
+                                              tstart, ntiles, g->stream));
+  HPGB_TRY(vb.sort_tmp.reserve(std::max(sort_bytes, scan_bytes) + 16));
+
+  HPGB_CUDA_TRY(cudaMemsetAsync(counts, 0, size_t(ntiles + 1) * 4, g->stream));
+  const unsigned blocks = unsigned((n + 255) / 256);
+  tile_keys_kernel<N><<<blocks, 256, 0, g->stream>>>(
+      static_cast<const VisData<N>*>(d_vis), n, geom, groups, tg,
+      vb.keys.as<unsigned>(), vb.order.as<unsigned>(), counts);
+  HPGB_CUDA_TRY(cudaGetLastError());
+  ++g->launches;
+  size_t tmp_bytes = vb.sort_tmp.bytes;
+  HPGB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(vb.sort_tmp.ptr, tmp_bytes, kbuf,
+                                                vbuf, int(n), 0, end_bit,
+                                                g->stream));
+  tmp_bytes = vb.sort_tmp.bytes;
+  HPGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(vb.sort_tmp.ptr, tmp_bytes, counts,
+                                              tstart, ntiles, g->stream));
+  const unsigned tblocks = unsigned((ntiles + 255) / 256);
+  chunk_count_kernel<<<tblocks, 256, 0, g->stream>>>(counts, ntiles, K, nch);
+  HPGB_CUDA_TRY(cudaGetLastError());
+  ++g->launches;
+  tmp_bytes = vb.sort_tmp.bytes;
+  HPGB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(vb.sort_tmp.ptr, tmp_bytes, nch,
+                                              cstart, ntiles, g->stream));
+  chunk_write_kernel<<<tblocks, 256, 0, g->stream>>>(
+      counts, tstart, nch, cstart, ntiles, K, vb.items.as<Chunk>(), num_chunks);
+  HPGB_CUDA_TRY(cudaGetLastError());
+  ++g->launches;
+  tile_desc_kernel<N><<<blocks, 256, 0, g->stream>>>(
+      static_cast<const VisData<N>*>(d_vis), vbuf.Current(), kbuf.Current(), n,
+      geom, groups, tg, g->cf.data.as<const float2>(), descs, srefs);
+  HPGB_CUDA_TRY(cudaGetLastError());
+  ++g->launches;
+
+  TiledParams p = plan.p;
+  p.descs = descs;
+  p.srefs = srefs;
+  p.chunks = vb.items.as<Chunk>();
+  p.num_chunks = num_chunks;
+  p.cf = g->cf.data.as<const float2>();
+  p.grid = g->grid.as<double2>();
+  p.weights = g->weights.as<double>();
+  p.records = static_cast<unsigned char*>(d_vis);
+  p.rec_stride = int(sizeof(VisData<N>));
+  p.status = vb.counters.as<unsigned>();
+
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  if (p.do_degrid && p.has_model) {
+    const void* base = g->model.ptr;
+    size_t esize = 8;
+    CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    if (mixed) {
+      const size_t ne = g->grid_elems();
+      if (!g->model32_valid) {
+        HPGB_TRY(g->model32.reserve(std::max<size_t>(ne, 1) * sizeof(float2)));
+        model_to_f32_kernel<<<148 * 8, 256, 0, g->stream>>>(
+            g->model.as<const double2>(), g->model32.as<float2>(), ne);
+        HPGB_CUDA_TRY(cudaGetLastError());
+        ++g->launches;
+        g->model32_valid = true;
+      }
+      base = g->model32.ptr;
+      esize = 4;
+      dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    }
+    auto enc = tensor_map_encoder();
+    if (!enc) return Status::err(HPGB_ERROR_OTHER, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[3] = {cuuint64_t(2 * p.nx), cuuint64_t(p.ny),
+                          cuuint64_t(p.nrow * p.ncube)};
+    cuuint64_t strides[2] = {cuuint64_t(2 * p.nx) * esize,
+                             cuuint64_t(2 * p.nx) * p.ny * esize};
+    cuuint32_t box[3] = {cuuint32_t(2 * p.R), cuuint32_t(p.R), 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(&map, dt, 3, const_cast<void*>(base), dims, strides, box,
+                     estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      return Status::err(HPGB_ERROR_OTHER,
+                         "cuTensorMapEncodeTiled failed: " + std::to_string(int(r)));
+  }
+  if (mixed) return launch_tiled<N, true>(g, p, plan.smem, map);
+  return launch_tiled<N, false>(g, p, plan.smem, map);
+}
+
+}  // namespace
+
+Status grid_tiled(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
+                  bool* used) {
+  *used = false;
+  if (n == 0) return Status::ok();
+  if (!(flags & (HPGB_DO_DEGRID | HPGB_DO_GRID))) {
+    *used = true;
+    return Status::ok();
+  }
+  if (n > size_t(0x7fffffff)) return Status::ok();
+  const bool mixed = g->precision == HPGB_PRECISION_MIXED;
+  const Plan plan = make_plan(g, flags, mixed);
+  if (!plan.ok) return Status::ok();
+  *used = true;
+  switch (g->npol) {
+    case 1: return grid_tiled_n<1>(g, d_vis, n, flags, plan, mixed);
+    case 2: return grid_tiled_n<2>(g, d_vis, n, flags, plan, mixed);
+    case 3: return grid_tiled_n<3>(g, d_vis, n, flags, plan, mixed);
+    case 4: return grid_tiled_n<4>(g, d_vis, n, flags, plan, mixed);
+    default: return Status::err(HPGB_ERROR_OTHER, "bad polarization count");
+  }
+}
+
+}  // namespace hpgb

@@ -67,6 +67,9 @@ struct hpgb_gridder {
   hpgb::DevBuf weights;   // double  [cube][mrow]
   hpgb::DevBuf model;     // double2, empty when no model is set
   bool has_model = false;
+  hpgb::DevBuf model32;   // float2 copy of the model for the mixed form
+  bool model32_valid = false;
+  int kernel_kind = HPGB_KERNEL_AUTO;
 
   hpgb::CFRegion cf;
   hpgb::VisBuffers vb;
@@ -98,6 +101,10 @@ Status set_cf(hpgb_gridder* g, unsigned os, unsigned ngroups,
               const unsigned* extents, const void* const* values, int layout,
               bool on_device);
 Status copy_cf(hpgb_gridder* dst, const hpgb_gridder* src);
+
+// grid_tiled.cu: *used is false when the tiled kernel cannot take the batch
+Status grid_tiled(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
+                  bool* used);
 
 // grid_direct.cu
 Status grid_direct(hpgb_gridder* g, const void* d_vis, size_t n,

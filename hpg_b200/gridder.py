@@ -152,6 +152,10 @@ class Gridder:
     def set_precision(self, precision):
         check(load().hpgb_set_precision(self._h, int(precision)))
 
+    def set_gridding_kernel(self, kind):
+        """abi.KERNEL_AUTO, KERNEL_DIRECT or KERNEL_TILED."""
+        check(load().hpgb_set_gridding_kernel(self._h, int(kind)))
+
     @property
     def stream(self):
         s = ctypes.c_void_p()

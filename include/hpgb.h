@@ -84,6 +84,18 @@ enum hpgb_shift_direction { HPGB_SHIFT_FORWARD = 0, HPGB_SHIFT_BACKWARD = 1 };
  *         weight sums stay FP64. */
 enum hpgb_precision { HPGB_PRECISION_FP64 = 0, HPGB_PRECISION_MIXED = 1 };
 
+/* Kernel family used by hpgb_grid_visibilities.
+ *  AUTO:   the tiled kernel when the CF fits its shared-memory ring, else
+ *          the per-visibility kernels.
+ *  DIRECT: per-visibility kernels with global FP64 atomics (the reference's
+ *          launch structure; FP64 form only).
+ *  TILED:  the tiled kernel, or an error when it cannot take the batch. */
+enum hpgb_kernel_kind {
+  HPGB_KERNEL_AUTO = 0,
+  HPGB_KERNEL_DIRECT = 1,
+  HPGB_KERNEL_TILED = 2
+};
+
 /* Layout of CF values handed to hpgb_set_cf (one buffer per CF group).
  *  LOGICAL: complex<float> indexed like CFArray::operator()(x, y, mueller,
  *           cube) (src/hpg.hpp:677-684), rightmost index fastest:
@@ -163,6 +175,10 @@ HPGB_API int hpgb_destroy(hpgb_gridder* gridder);
 
 /* Select the arithmetic form (enum hpgb_precision) of later gridding calls. */
 HPGB_API int hpgb_set_precision(hpgb_gridder* gridder, int precision);
+
+/* Select the kernel family (enum hpgb_kernel_kind) of later gridding calls;
+ * no counterpart in the reference. */
+HPGB_API int hpgb_set_gridding_kernel(hpgb_gridder* gridder, int kind);
 
 /* The CUDA stream (cudaStream_t) all work of this gridder is issued on. */
 HPGB_API int hpgb_get_stream(const hpgb_gridder* gridder, void** stream);
