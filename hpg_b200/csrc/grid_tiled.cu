@@ -30,8 +30,9 @@
 //                           distributed shared memory and a remote mbarrier,
 //                           form the prediction and residual (identically in
 //                           every CTA), and grid the scaled residual into the
-//                           row's shared-memory grid tile; the gridding of
-//                           visibility j overlaps the exchange of j+1;
+//                           row's shared-memory grid tile; visibility j is
+//                           finished and gridded while the partials of j+1
+//                           travel (four exchange buffers in flight);
 //                         - at the end of a chunk the tile is added to the
 //                           FP64 grid with red.global.add.f64, and the row's
 //                           weight sum to the weights.
@@ -61,12 +62,22 @@
 
 namespace hpgb {
 
+#ifdef HPGB_TILED_TIMERS
+unsigned long long* g_tiled_timers = nullptr;
+#endif
+
 namespace {
 
-constexpr int kConsumerWarps = 8;
-constexpr int kConsumers = kConsumerWarps * 32;
+// warp roles of the tiled kernel: kDG degridding warps, one exchange warp,
+// kGR gridding warps, one producer warp
+constexpr int kDG = 8;
+constexpr int kGR = 8;
+constexpr int kXWarp = kDG;
+constexpr int kGRBase = kDG + 1;
+constexpr int kPWarp = kGRBase + kGR;
+constexpr int kConsumers = (kDG + 1 + kGR) * 32;
 constexpr int kThreadsTiled = kConsumers + 32;
-constexpr int kMaxSlots = 4;
+constexpr int kSlots = 8;  // descriptor slots (visibilities in flight)
 constexpr int kChunkVisFP64 = 2048;
 constexpr int kChunkVisMixed = 256;
 constexpr int kMaxRuns = 8;
@@ -80,7 +91,7 @@ struct alignas(16) TileDesc {
   double phi0[2], dphi[2];
   float2 vals[4];
   float weights[4];
-  double2 den[4];        // degridding normaliser per polarization
+  double2 wfac[4];       // conj(phasor) / normaliser, per polarization
   double twgt[4];        // grid weight increment per grid row
   float2 gvis[4];        // values scaled for gridding (used without degrid)
   int32_t pad1[4];
@@ -102,7 +113,7 @@ struct Chunk {
 struct TiledParams {
   int nx, ny, nrow, ncube;
   int R, T, ntx, nty;
-  int D, slot_bytes, model_bytes;
+  int ring_bytes, model_bytes;  // CF ring size (bytes, multiple of 128)
   int esize_model, esize_grid;  // bytes per tile element; 0 when unused
   int nplanes[4];
   int nruns[4];
@@ -122,25 +133,48 @@ struct TiledParams {
   unsigned char* records;  // VisData<N> records (values written back)
   int rec_stride;
   unsigned* status;
+  unsigned long long* timers;  // per-CTA phase cycle counters (timer builds)
 };
 
+// Phase timers: compiled in only with -DHPGB_TILED_TIMERS (measurement
+// builds); they record clock64() intervals per CTA, nothing else changes.
+#ifdef HPGB_TILED_TIMERS
+#define TT_DECL(n) unsigned long long tt_[n] = {0}; long long tt0_ = 0
+#define TT_BEGIN() tt0_ = clock64()
+#define TT_END(i) tt_[i] += (unsigned long long)(clock64() - tt0_)
+#define TT_STORE(base, n)                                              \
+  for (int i_ = 0; i_ < (n); ++i_)                                     \
+    if (p.timers) atomicAdd(&p.timers[(base) + i_], tt_[i_])
+#define TT_PUT(slot, i) \
+  if (p.timers) atomicAdd(&p.timers[blockIdx.x * 16 + (slot)], tt_[i])
+#else
+#define TT_PUT(slot, i)
+#define TT_DECL(n)
+#define TT_BEGIN()
+#define TT_END(i)
+#define TT_STORE(base, n)
+#endif
+
 struct SmemLayout {
-  int bars, xbuf, wred, bcast, desc, ring, model, grid, total;
+  int bars, xbuf, wred, bcast, slots, desc, ring, model, grid, total;
 };
 
 __host__ __device__ inline int align_up(int v, int a) { return (v + a - 1) / a * a; }
 
-__host__ __device__ inline SmemLayout smem_layout(int D, int slot_bytes, int R,
+__host__ __device__ inline SmemLayout smem_layout(int ring_bytes, int R,
                                                   int esize_model,
                                                   int esize_grid) {
   SmemLayout L;
-  L.bars = 0;                       // 16 mbarriers
-  L.xbuf = 128;                     // [2][4 rows][4 pol] complex double
-  L.wred = L.xbuf + 2 * 4 * 4 * 16; // [warps][8] double
-  L.bcast = L.wred + kConsumerWarps * 8 * 8;  // [2][4] float2
-  L.desc = align_up(L.bcast + 2 * 4 * 8, 128);
-  L.ring = align_up(L.desc + kMaxSlots * int(sizeof(TileDesc)), 1024);
-  L.model = align_up(L.ring + D * slot_bytes, 1024);
+  // 33 mbarriers: full[8] empty[8] model xchg[4] dgfull[2] dgempty[2]
+  // gvfull[8], then the abort flag
+  L.bars = 0;
+  L.xbuf = 320;                       // [4][4 rows][4 pol] complex double
+  L.wred = L.xbuf + 4 * 4 * 4 * 16;   // [2][kDG][8] double (degrid partials)
+  L.bcast = L.wred + 2 * kDG * 8 * 8; // [kSlots][4] float2 (gridding values)
+  L.slots = L.bcast + kSlots * 4 * 8;  // ring_off[kSlots] int, slot_end[kSlots] u64
+  L.desc = align_up(L.slots + kSlots * 4 + kSlots * 8, 128);
+  L.ring = align_up(L.desc + kSlots * int(sizeof(TileDesc)), 1024);
+  L.model = align_up(L.ring + ring_bytes, 1024);
   L.grid = align_up(L.model + R * R * esize_model, 128);
   L.total = L.grid + R * R * esize_grid;
   return L;
@@ -253,7 +287,10 @@ __global__ void tile_desc_kernel(const VisData<N>* vis, const unsigned* order,
           den = cadd_d(den, make_double2(w.x, vc.pos_w ? w.y : -w.y));
         }
       }
-    d.den[v] = den;
+    // prediction = sum * conj(phasor) / normaliser (src/hpg_core.hpp:670-679),
+    // with the factor formed here once per visibility
+    if (den.x == 0.0 && den.y == 0.0) den = make_double2(1.0, 0.0);
+    d.wfac[v] = cdiv_d(make_double2(d.phasor.x, -d.phasor.y), den);
   }
   // grid weight per row: sum_vpol |sum_XY cf| * w (src/hpg_core.hpp:877-885)
   for (int r = 0; r < 4; ++r) {
@@ -304,23 +341,28 @@ struct Form<true> {
   using grid_t = float2;
 };
 
+// Partial degridding sums of row `row` over the cells c = first, first +
+// stride, ... of one visibility's footprint (src/hpg_core.hpp:642-668).
 template <int N, bool MIXED>
-__device__ __forceinline__ void degrid_cells(const TiledParams& p,
-                                             const TileDesc& d,
-                                             const float2* cfs, int row,
-                                             const typename Form<MIXED>::model_t* mtile,
-                                             int ctid, double (&acc)[2 * N]) {
+__device__ __forceinline__ void degrid_cells(
+    const TiledParams& p, const TileDesc& d, const float2* cfs, int row,
+    const typename Form<MIXED>::model_t* mtile, int first, int stride,
+    double (&acc)[2 * N]) {
   const bool pos_w = d.flags & kPosW;
   const bool screen_on = d.flags & kScreen;
   const int tx = d.taps_x, ncell = int(d.taps_x) * d.taps_y;
+  const int pst = d.pstride, R = p.R;
   const float im = pos_w ? 1.0f : -1.0f;
   int pp[N];
 #pragma unroll
   for (int v = 0; v < N; ++v) pp[v] = p.dpos[row][pos_w ? 1 : 0][v];
+  // (X, Y) of cell `first`, advanced incrementally
+  int Y = first / tx, X = first - Y * tx;
+  const int dY = stride / tx, dX = stride - dY * tx;
+  const typename Form<MIXED>::model_t* mrow = mtile + d.cy * R + d.cx;
   if constexpr (!MIXED) {
-    for (int c = ctid; c < ncell; c += kConsumers) {
-      const int Y = c / tx, X = c - Y * tx;
-      double2 mv = mtile[(d.cy + Y) * p.R + d.cx + X];
+    for (int c = first; c < ncell; c += stride) {
+      double2 mv = mrow[Y * R + X];
       if (screen_on) {
         const double phx = __dadd_rn(d.phi0[0], __dmul_rn(double(X), d.dphi[0]));
         const double phy = __dadd_rn(d.phi0[1], __dmul_rn(double(Y), d.dphi[1]));
@@ -329,20 +371,25 @@ __device__ __forceinline__ void degrid_cells(const TiledParams& p,
 #pragma unroll
       for (int v = 0; v < N; ++v) {
         if (pp[v] >= 0) {
-          const float2 cf = cfs[pp[v] * d.pstride + c];
-          const double cr = cf.x, ci = double(cf.y) * im;
+          const float2 cf = cfs[pp[v] * pst + c];
+          const double cr = cf.x, ci = double(cf.y * im);
           acc[2 * v] = fma(cr, mv.x, fma(-ci, mv.y, acc[2 * v]));
           acc[2 * v + 1] = fma(cr, mv.y, fma(ci, mv.x, acc[2 * v + 1]));
         }
+      }
+      X += dX;
+      Y += dY;
+      if (X >= tx) {
+        X -= tx;
+        ++Y;
       }
     }
   } else {
     float a[2 * N];
 #pragma unroll
     for (int k = 0; k < 2 * N; ++k) a[k] = 0.f;
-    for (int c = ctid; c < ncell; c += kConsumers) {
-      const int Y = c / tx, X = c - Y * tx;
-      float2 mv = mtile[(d.cy + Y) * p.R + d.cx + X];
+    for (int c = first; c < ncell; c += stride) {
+      float2 mv = mrow[Y * R + X];
       if (screen_on) {
         const double phx = __dadd_rn(d.phi0[0], __dmul_rn(double(X), d.dphi[0]));
         const double phy = __dadd_rn(d.phi0[1], __dmul_rn(double(Y), d.dphi[1]));
@@ -353,11 +400,17 @@ __device__ __forceinline__ void degrid_cells(const TiledParams& p,
 #pragma unroll
       for (int v = 0; v < N; ++v) {
         if (pp[v] >= 0) {
-          const float2 cf = cfs[pp[v] * d.pstride + c];
+          const float2 cf = cfs[pp[v] * pst + c];
           const float ci = cf.y * im;
           a[2 * v] = fmaf(cf.x, mv.x, fmaf(-ci, mv.y, a[2 * v]));
           a[2 * v + 1] = fmaf(cf.x, mv.y, fmaf(ci, mv.x, a[2 * v + 1]));
         }
+      }
+      X += dX;
+      Y += dY;
+      if (X >= tx) {
+        X -= tx;
+        ++Y;
       }
     }
 #pragma unroll
@@ -365,16 +418,24 @@ __device__ __forceinline__ void degrid_cells(const TiledParams& p,
   }
 }
 
+// Gridding of one visibility into the rows of the grid tile owned by warp
+// `gw` (tile rows congruent to gw modulo kGR), so that different warps never
+// write the same tile cell (src/hpg_core.hpp:856-873).
 template <int N, bool MIXED>
-__device__ __forceinline__ void grid_cells(const TiledParams& p,
-                                           const TileDesc& d, const float2* cfs,
-                                           int row, const float2* gvis,
-                                           typename Form<MIXED>::grid_t* gtile,
-                                           int ctid) {
+__device__ __forceinline__ void grid_rows(const TiledParams& p,
+                                          const TileDesc& d, const float2* cfs,
+                                          int row, const float2* gvis,
+                                          typename Form<MIXED>::grid_t* gtile,
+                                          int gw, int lane) {
   const bool pos_w = d.flags & kPosW;
   const bool screen_on = d.flags & kScreen;
-  const int tx = d.taps_x, ncell = int(d.taps_x) * d.taps_y;
+  const int tx = d.taps_x, ty = d.taps_y;
+  const int pst = d.pstride, R = p.R;
   const float im = pos_w ? -1.0f : 1.0f;
+  const int Y0 = (gw - d.cy % kGR + kGR) % kGR;  // first footprint row owned
+  if (Y0 >= ty) return;
+  const int nr = (ty - Y0 + kGR - 1) / kGR;
+  const int ncw = nr * tx;  // cells of this warp
   int pp[N];
   float2 gv[N];
 #pragma unroll
@@ -382,8 +443,13 @@ __device__ __forceinline__ void grid_cells(const TiledParams& p,
     pp[v] = p.gpos[row][pos_w ? 1 : 0][v];
     gv[v] = gvis[v];
   }
-  for (int c = ctid; c < ncell; c += kConsumers) {
-    const int Y = c / tx, X = c - Y * tx;
+  // flattened index i -> (row r_i, X); footprint row Y = Y0 + r_i*kGR
+  int ri = lane / tx, X = lane - ri * tx;
+  const int dR = 32 / tx, dX = 32 - dR * tx;
+  typename Form<MIXED>::grid_t* gbase = gtile + d.cy * R + d.cx;
+  for (int i = lane; i < ncw; i += 32) {
+    const int Y = Y0 + ri * kGR;
+    const int c = Y * tx + X;
     float2 screen = make_float2(1.0f, 0.0f);
     if (screen_on) {
       const double phx = __dadd_rn(d.phi0[0], __dmul_rn(double(X), d.dphi[0]));
@@ -391,13 +457,13 @@ __device__ __forceinline__ void grid_cells(const TiledParams& p,
       const double2 s = cphase_d(__dadd_rn(phx, phy));
       screen = make_float2(__double2float_rn(s.x), __double2float_rn(s.y));
     }
-    const int idx = (d.cy + Y) * p.R + d.cx + X;
+    const int idx = Y * R + X;
     if constexpr (!MIXED) {
       double sx = 0.0, sy = 0.0;
 #pragma unroll
       for (int v = 0; v < N; ++v) {
         if (pp[v] >= 0) {
-          float2 cf = cfs[pp[v] * d.pstride + c];
+          float2 cf = cfs[pp[v] * pst + c];
           cf.y *= im;
           const float2 prod =
               screen_on ? cmul_f(cmul_f(cf, screen), gv[v]) : cmul_f(cf, gv[v]);
@@ -405,16 +471,16 @@ __device__ __forceinline__ void grid_cells(const TiledParams& p,
           sy = __dadd_rn(sy, double(prod.y));
         }
       }
-      double2 t = gtile[idx];
+      double2 t = gbase[idx];
       t.x += sx;
       t.y += sy;
-      gtile[idx] = t;
+      gbase[idx] = t;
     } else {
       float sx = 0.f, sy = 0.f;
 #pragma unroll
       for (int v = 0; v < N; ++v) {
         if (pp[v] >= 0) {
-          float2 cf = cfs[pp[v] * d.pstride + c];
+          float2 cf = cfs[pp[v] * pst + c];
           cf.y *= im;
           if (screen_on)
             cf = make_float2(cf.x * screen.x - cf.y * screen.y,
@@ -423,10 +489,16 @@ __device__ __forceinline__ void grid_cells(const TiledParams& p,
           sy = fmaf(cf.x, gv[v].y, fmaf(cf.y, gv[v].x, sy));
         }
       }
-      float2 t = gtile[idx];
+      float2 t = gbase[idx];
       t.x += sx;
       t.y += sy;
-      gtile[idx] = t;
+      gbase[idx] = t;
+    }
+    X += dX;
+    ri += dR;
+    if (X >= tx) {
+      X -= tx;
+      ++ri;
     }
   }
 }
@@ -443,14 +515,24 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       sm_raw + ((1024u - (ptx::smem(sm_raw) & 1023u)) & 1023u);
   // same layout the host sized the launch with (tiles absent when unused)
   const SmemLayout L =
-      smem_layout(p.D, p.slot_bytes, p.R, p.esize_model, p.esize_grid);
+      smem_layout(p.ring_bytes, p.R, p.esize_model, p.esize_grid);
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + L.bars);
-  uint64_t* empty = full + kMaxSlots;
-  uint64_t* model_bar = full + 2 * kMaxSlots;
-  uint64_t* xchg = model_bar + 1;
-  double* xbuf = reinterpret_cast<double*>(sm + L.xbuf);  // [2][4][4][2]
-  double* wred = reinterpret_cast<double*>(sm + L.wred);  // [warps][8]
-  float2* bcast = reinterpret_cast<float2*>(sm + L.bcast);  // [2][4]
+  uint64_t* empty = full + kSlots;
+  uint64_t* model_bar = empty + kSlots;
+  uint64_t* xchg = model_bar + 1;  // [4]
+  uint64_t* dgfull = xchg + 4;     // [2]
+  uint64_t* dgempty = dgfull + 2;  // [2]
+  uint64_t* gvfull = dgempty + 2;  // [kSlots]
+  volatile int* abort = reinterpret_cast<volatile int*>(gvfull + kSlots);
+  double* xbuf = reinterpret_cast<double*>(sm + L.xbuf);  // [4][4][4][2]
+  double* dgpart = reinterpret_cast<double*>(sm + L.wred);  // [2][kDG][8]
+  // gridding values of visibility q in entry q % kSlots: the exchange warp
+  // runs at most kSlots - 1 visibilities ahead of the gridding warps (the
+  // producer reclaims a slot only after they are done with it)
+  float2* gvring = reinterpret_cast<float2*>(sm + L.bcast);  // [kSlots][4]
+  int* ring_off = reinterpret_cast<int*>(sm + L.slots);  // [kSlots]
+  unsigned long long* slot_end =
+      reinterpret_cast<unsigned long long*>(sm + L.slots + kSlots * 4);
   TileDesc* descs = reinterpret_cast<TileDesc*>(sm + L.desc);
   unsigned char* ring = sm + L.ring;
   MT* mtile = reinterpret_cast<MT*>(sm + L.model);
@@ -460,67 +542,134 @@ tiled_kernel(const __grid_constant__ TiledParams p,
   const int warp = tid >> 5, lane = tid & 31;
   const int row = int(ptx::cluster_rank());
   const unsigned cid = ptx::cluster_id_x(), ncl = ptx::num_clusters_x();
+  const bool exchange = p.do_degrid && p.has_model;
+  // every role that reads a ring slot releases it
+  const uint32_t empty_count = uint32_t((exchange ? kDG : 0) + 1 + kGR);
 
   if (tid == 0) {
-    for (int s = 0; s < p.D; ++s) {
+    for (int s = 0; s < kSlots; ++s) {
       ptx::mbar_init(&full[s], 1);
-      ptx::mbar_init(&empty[s], kConsumerWarps);
+      ptx::mbar_init(&empty[s], empty_count);
     }
     ptx::mbar_init(model_bar, 1);
-    ptx::mbar_init(&xchg[0], uint32_t(p.nrow));
-    ptx::mbar_init(&xchg[1], uint32_t(p.nrow));
+    for (int x = 0; x < 4; ++x) ptx::mbar_init(&xchg[x], 1);
+    for (int x = 0; x < 2; ++x) {
+      ptx::mbar_init(&dgfull[x], kDG);
+      ptx::mbar_init(&dgempty[x], 1);
+    }
+    for (int x = 0; x < kSlots; ++x) ptx::mbar_init(&gvfull[x], 1);
+    *abort = 0;
     ptx::fence_mbar_init();
   }
   __syncthreads();
-  ptx::cluster_sync();  // every CTA's barriers exist before remote arrivals
+  ptx::cluster_sync();  // every CTA's barriers exist before remote traffic
 
   const unsigned nchunks = *p.num_chunks;
   bool ok = true;
-  const bool exchange = p.do_degrid && p.has_model;
+  const int RR = p.R * p.R;
 
-  if (warp == kConsumerWarps) {
-    // ---------------- producer ----------------
-    if (lane == 0) {
-      uint32_t q = 0;
-      for (unsigned c = cid; c < nchunks; c += ncl) {
-        const Chunk ch = p.chunks[c];
-        for (int k = 0; k < ch.count; ++k, ++q) {
-          const int s = int(q % uint32_t(p.D));
-          if (q >= uint32_t(p.D))
-            ok &= ptx::mbar_wait(&empty[s], ((q / p.D) & 1) ^ 1);
-          const int j = ch.start + k;
-          const SliceRef sr = p.srefs[j];
-          const uint32_t pbytes = uint32_t(sr.pstride) * 8u;
-          const uint32_t bytes =
-              uint32_t(sizeof(TileDesc)) + uint32_t(p.nplanes[row]) * pbytes;
-          ptx::mbar_expect_tx(&full[s], bytes);
-          ptx::bulk_g2s(&descs[s], &p.descs[j], uint32_t(sizeof(TileDesc)),
-                        &full[s]);
-          unsigned char* dst = ring + size_t(s) * p.slot_bytes;
-          const float2* slice = p.cf + sr.off;
-          for (int u = 0; u < p.nruns[row]; ++u)
-            ptx::bulk_g2s(dst + p.run_dst[row][u] * pbytes,
-                          slice + size_t(p.run_plane[row][u]) * sr.pstride,
-                          uint32_t(p.run_len[row][u]) * pbytes, &full[s]);
-          // pull the slice of a later visibility of this chunk into L2
-          const int kp = k + p.D + 2;
-          if (kp < ch.count) {
-            const SliceRef sp = p.srefs[ch.start + kp];
-            const uint32_t pb = uint32_t(sp.pstride) * 8u;
-            const float2* sl = p.cf + sp.off;
-            for (int u = 0; u < p.nruns[row]; ++u)
-              ptx::bulk_prefetch_l2(sl + size_t(p.run_plane[row][u]) * sp.pstride,
-                                    uint32_t(p.run_len[row][u]) * pb);
-          }
+  if (warp == kPWarp) {
+    // ---------------- producer warp ----------------
+    // Lane k holds the slice references of visibilities base+k and
+    // base+32+k of the current chunk; per visibility the warp reserves a
+    // descriptor slot and room in the byte ring, and lane 0 issues the bulk
+    // copies of its descriptor and of the CF planes of this CTA's row and
+    // pulls the slice of the visibility kPrefetch places ahead into L2.
+    constexpr int kPrefetch = 16;  // < 32, so the window cur/nxt covers it
+    uint32_t q = 0;
+    uint32_t q_old = 0;               // oldest visibility not yet reclaimed
+    unsigned long long head = 0;      // ring bytes allocated (monotonic)
+    unsigned long long tail = 0;      // ring bytes released (monotonic)
+    TT_DECL(2);
+    for (unsigned c = cid; c < nchunks; c += ncl) {
+      const Chunk ch = p.chunks[c];
+      SliceRef cur{}, nxt{};
+      if (lane < ch.count) cur = p.srefs[ch.start + lane];
+      if (32 + lane < ch.count) nxt = p.srefs[ch.start + 32 + lane];
+      for (int k = 0; k < ch.count; ++k, ++q) {
+        if (k > 0 && (k & 31) == 0) {
+          cur = nxt;
+          nxt = SliceRef{};
+          if (k + 32 + lane < ch.count) nxt = p.srefs[ch.start + k + 32 + lane];
         }
+        const int kk = k & 31;
+        const long long off = __shfl_sync(0xffffffffu, cur.off, kk);
+        const int pstride = __shfl_sync(0xffffffffu, cur.pstride, kk);
+        const int kp = kk + kPrefetch;  // < 64
+        const long long poff = kp < 32 ? __shfl_sync(0xffffffffu, cur.off, kp & 31)
+                                       : __shfl_sync(0xffffffffu, nxt.off, kp & 31);
+        const int ppst = kp < 32 ? __shfl_sync(0xffffffffu, cur.pstride, kp & 31)
+                                 : __shfl_sync(0xffffffffu, nxt.pstride, kp & 31);
+        // Reclaim the oldest visibilities' slots until a descriptor slot
+        // is free and the CF part fits in the byte ring (allocations never
+        // straddle the ring end; they are released in order).
+        const bool cf_needed = exchange || p.do_grid;
+        const uint32_t pbytes = uint32_t(pstride) * 8u;
+        const unsigned long long need =
+            cf_needed ? (unsigned long long)(p.nplanes[row]) * pbytes : 0ull;
+        TT_BEGIN();
+        for (;;) {
+          unsigned long long h = head;
+          const unsigned long long pos = h % (unsigned long long)p.ring_bytes;
+          if (need > 0 && pos + need > (unsigned long long)p.ring_bytes)
+            h += (unsigned long long)p.ring_bytes - pos;
+          const bool need_slot = (q - q_old) >= uint32_t(kSlots);
+          const bool need_space =
+              need > 0 && h + need - tail > (unsigned long long)p.ring_bytes;
+          if (!need_slot && !need_space) {
+            head = h;
+            break;
+          }
+          if (q_old == q) {  // cannot happen: the plan keeps need <= ring
+            ok = false;
+            break;
+          }
+          const int so = int(q_old % uint32_t(kSlots));
+          ok &= ptx::mbar_wait(&empty[so], (q_old / kSlots) & 1, abort);
+          tail = slot_end[so];
+          ++q_old;
+        }
+        TT_END(0);
+        const int s = int(q % uint32_t(kSlots));
+        // after an abort nothing is copied into slots that may still be read
+        if (lane == 0 && !*abort) {
+          TT_BEGIN();
+          const int roff = int(head % (unsigned long long)p.ring_bytes);
+          ring_off[s] = roff;
+          slot_end[s] = head + need;
+          ptx::mbar_expect_tx(&full[s], uint32_t(sizeof(TileDesc)) + uint32_t(need));
+          ptx::bulk_g2s(&descs[s], &p.descs[ch.start + k],
+                        uint32_t(sizeof(TileDesc)), &full[s]);
+          if (cf_needed) {
+            unsigned char* dst = ring + roff;
+            const float2* slice = p.cf + off;
+            for (int u = 0; u < p.nruns[row]; ++u)
+              ptx::bulk_g2s(dst + p.run_dst[row][u] * pbytes,
+                            slice + size_t(p.run_plane[row][u]) * pstride,
+                            uint32_t(p.run_len[row][u]) * pbytes, &full[s]);
+            if (k + kPrefetch < ch.count) {
+              const float2* sl = p.cf + poff;
+              const uint32_t pb = uint32_t(ppst) * 8u;
+              for (int u = 0; u < p.nruns[row]; ++u)
+                ptx::bulk_prefetch_l2(sl + size_t(p.run_plane[row][u]) * ppst,
+                                      uint32_t(p.run_len[row][u]) * pb);
+            }
+          }
+          TT_END(1);
+        }
+        head += need;
+        __syncwarp();
       }
     }
+    if (lane == 0) { TT_STORE(blockIdx.x * 16 + 12, 2); }
   } else {
-    // ---------------- consumers ----------------
-    const int ctid = tid;
+    // ---------------- consumer roles ----------------
+    // degridding warps [0, kDG), exchange warp kXWarp, gridding warps
+    // [kGRBase, kGRBase + kGR).  Roles hand visibilities to each other
+    // through mbarriers; all of them meet at chunk boundaries.
     uint32_t q = 0;
     uint32_t model_phase = 0;
-    const int RR = p.R * p.R;
+    TT_DECL(10);
     for (unsigned c = cid; c < nchunks; c += ncl) {
       const Chunk ch = p.chunks[c];
       const int tile = ch.tile;
@@ -528,8 +677,9 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       const int ty = (tile / p.ntx) % p.nty;
       const int cube = tile / (p.ntx * p.nty);
       const int x0 = tx * p.T, y0 = ty * p.T;
+      TT_BEGIN();
       ptx::named_sync(1, kConsumers);
-      if (exchange && ctid == 0) {
+      if (exchange && tid == 0 && !*abort) {
         // earlier generic-proxy reads of the tile precede this async write
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         ptx::mbar_expect_tx(model_bar, uint32_t(p.model_bytes));
@@ -537,135 +687,183 @@ tiled_kernel(const __grid_constant__ TiledParams p,
                          model_bar);
       }
       if (p.do_grid)
-        for (int i = ctid; i < RR; i += kConsumers) {
+        for (int i = tid; i < RR; i += kConsumers) {
           GT z;
           z.x = 0;
           z.y = 0;
           gtile[i] = z;
         }
       if (exchange) {
-        ok &= ptx::mbar_wait(model_bar, model_phase);
+        ok &= ptx::mbar_wait(model_bar, model_phase, abort);
         model_phase ^= 1;
       }
       ptx::named_sync(1, kConsumers);
+      TT_END(0);
       double wchunk = 0.0;
-      int prev_s = -1;
-      for (int k = 0; k < ch.count; ++k, ++q) {
-        const int s = int(q % uint32_t(p.D));
-        ok &= ptx::mbar_wait(&full[s], (q / p.D) & 1);
-        const TileDesc& d = descs[s];
-        const float2* cfs =
-            reinterpret_cast<const float2*>(ring + size_t(s) * p.slot_bytes);
-        const int xs = int(q & 1);
-        if (exchange) {
+
+      if (warp < kDG) {
+        // -------- degridding warps --------
+        for (int k = 0; k < ch.count; ++k, ++q) {
+          const int s = int(q % uint32_t(kSlots));
+          if (!exchange) continue;
+          TT_BEGIN();
+          ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
+          TT_END(1);
+          if (ptx::warp_flag(abort)) continue;
+          TT_BEGIN();
           double acc[2 * N];
 #pragma unroll
           for (int t = 0; t < 2 * N; ++t) acc[t] = 0.0;
-          degrid_cells<N, MIXED>(p, d, cfs, row, mtile, ctid, acc);
+          degrid_cells<N, MIXED>(
+              p, descs[s],
+              reinterpret_cast<const float2*>(ring + ring_off[s]),
+              row, mtile, warp * 32 + lane, kDG * 32, acc);
 #pragma unroll
           for (int t = 0; t < 2 * N; ++t) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1)
               acc[t] += __shfl_down_sync(0xffffffffu, acc[t], o);
           }
+          TT_END(2);
+          const int b = int(q & 1);
+          if (q >= 2) ok &= ptx::mbar_wait(&dgempty[b], ((q >> 1) & 1) ^ 1, abort);
+          if (ptx::warp_flag(abort)) continue;
           if (lane == 0) {
 #pragma unroll
-            for (int t = 0; t < 2 * N; ++t) wred[warp * 8 + t] = acc[t];
+            for (int t = 0; t < 2 * N; ++t) dgpart[(b * kDG + warp) * 8 + t] = acc[t];
+            ptx::mbar_arrive(&dgfull[b]);
+            ptx::mbar_arrive(&empty[s]);
           }
-          ptx::named_sync(2, kConsumers);
-          if (ctid == 0) {
-            double tot[2 * N];
-#pragma unroll
-            for (int t = 0; t < 2 * N; ++t) {
-              double sum = wred[t];
-              for (int w = 1; w < kConsumerWarps; ++w) sum += wred[w * 8 + t];
-              tot[t] = sum;
-            }
-            // partials of row `row` into every CTA of the cluster
-            for (int r = 0; r < p.nrow; ++r) {
-#pragma unroll
-              for (int t = 0; t < 2 * N; ++t)
-                ptx::st_cluster_f64(&xbuf[((xs * 4 + row) * 4) * 2 + t],
-                                    uint32_t(r), tot[t]);
-            }
-            for (int r = 0; r < p.nrow; ++r)
-              ptx::mbar_arrive_remote(&xchg[xs], uint32_t(r));
-          }
-        }
-        // grid the previous visibility while the exchange completes
-        if (prev_s >= 0) {
-          if (p.do_grid)
-            grid_cells<N, MIXED>(p, descs[prev_s],
-                                 reinterpret_cast<const float2*>(
-                                     ring + size_t(prev_s) * p.slot_bytes),
-                                 row, &bcast[(xs ^ 1) * 4], gtile, ctid);
           __syncwarp();
-          if (lane == 0) ptx::mbar_arrive(&empty[prev_s]);
         }
-        if (ctid == 0) {
-          float2 gout[4];
-          if (p.do_degrid) {
-            float2 pred[4];
-            if (exchange) {
-              ok &= ptx::mbar_wait_cluster(&xchg[xs], (q >> 1) & 1);
-              const double2 cph = make_double2(d.phasor.x, -d.phasor.y);
-#pragma unroll
-              for (int v = 0; v < N; ++v) {
-                double2 num = make_double2(0.0, 0.0);
-                for (int r = 0; r < p.nrow; ++r) {
-                  const double* x = &xbuf[((xs * 4 + r) * 4) * 2];
-                  num.x += x[2 * v];
-                  num.y += x[2 * v + 1];
+      } else if (warp == kXWarp) {
+        // -------- exchange warp --------
+        // Step k sends the row partials of visibility q (k < count) and then
+        // finishes visibility q-1, whose partials from the other rows were
+        // sent one step earlier and have normally arrived by now.
+        int prev_s = -1;
+        for (int k = 0; k <= ch.count; ++k) {
+          int s = -1;
+          if (k < ch.count) {
+            s = int(q % uint32_t(kSlots));
+            TT_BEGIN();
+            ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
+            TT_END(1);
+            if (exchange && !ptx::warp_flag(abort)) {
+              TT_BEGIN();
+              const int xs = int(q & 3);
+              const int b = int(q & 1);
+              TT_END(4);
+              TT_BEGIN();
+              ok &= ptx::mbar_wait(&dgfull[b], (q >> 1) & 1, abort);
+              TT_END(2);
+              TT_BEGIN();
+              const bool live = !ptx::warp_flag(abort);
+              double tot = 0.0;
+              if (live && lane < 2 * N)
+                for (int w = 0; w < kDG; ++w) tot += dgpart[(b * kDG + w) * 8 + lane];
+              __syncwarp();
+              if (live && lane == 0) {
+                ptx::mbar_arrive(&dgempty[b]);
+                // this CTA expects every row's partials for visibility q
+                ptx::mbar_expect_tx(&xchg[xs], uint32_t(p.nrow * 2 * N * 8));
+              }
+              // lane r*2N + t sends component t of this row's partial to CTA r
+              const int r = lane / (2 * N), t = lane % (2 * N);
+              const double v = __shfl_sync(0xffffffffu, tot, t);
+              if (live && r < p.nrow)
+                ptx::st_async_f64(&xbuf[((xs * 4 + row) * 4) * 2 + t],
+                                  uint32_t(r), v, &xchg[xs]);
+              TT_END(4);
+            }
+          }
+          if (prev_s >= 0) {
+            TT_BEGIN();
+            const uint32_t qq = q - 1;
+            const TileDesc& d = descs[prev_s];
+            const int xs = int(qq & 3);
+            const int gs = int(qq % uint32_t(kSlots));
+            TT_END(5);
+            TT_BEGIN();
+            if (exchange) ok &= ptx::mbar_wait_cluster(&xchg[xs], (qq >> 2) & 1, abort);
+            TT_END(3);
+            TT_BEGIN();
+            const bool live = !ptx::warp_flag(abort);
+            float2 gout = make_float2(0.f, 0.f);
+            if (live && lane < N) {
+              const int v = lane;
+              if (p.do_degrid) {
+                float2 pred = make_float2(0.f, 0.f);
+                if (exchange) {
+                  double2 num = make_double2(0.0, 0.0);
+                  for (int r = 0; r < p.nrow; ++r) {
+                    const double* x = &xbuf[((xs * 4 + r) * 4 + v) * 2];
+                    num.x += x[0];
+                    num.y += x[1];
+                  }
+                  const double2 qv = cmul_d(num, d.wfac[v]);
+                  pred = make_float2(__double2float_rn(qv.x),
+                                     __double2float_rn(qv.y));
                 }
-                double2 den = d.den[v];
-                if (den.x == 0.0 && den.y == 0.0) den = make_double2(1.0, 0.0);
-                const double2 qv = cmul_d(cdiv_d(num, den), cph);
-                pred[v] = make_float2(__double2float_rn(qv.x),
-                                      __double2float_rn(qv.y));
-              }
-            } else {
-#pragma unroll
-              for (int v = 0; v < N; ++v) pred[v] = make_float2(0.f, 0.f);
-            }
-            float2* out = reinterpret_cast<float2*>(
-                p.records + size_t(d.index) * p.rec_stride);
-#pragma unroll
-            for (int v = 0; v < N; ++v) {
-              if (p.do_grid) {
-                const float2 r = make_float2(__fsub_rn(d.vals[v].x, pred[v].x),
-                                             __fsub_rn(d.vals[v].y, pred[v].y));
-                if (row == 0) out[v] = r;
-                gout[v] = scale_for_gridding(r, d.phasor, d.weights[v]);
+                float2* out = reinterpret_cast<float2*>(
+                    p.records + size_t(d.index) * p.rec_stride);
+                if (p.do_grid) {
+                  const float2 rr = make_float2(__fsub_rn(d.vals[v].x, pred.x),
+                                                __fsub_rn(d.vals[v].y, pred.y));
+                  if (row == 0) out[v] = rr;
+                  gout = scale_for_gridding(rr, d.phasor, d.weights[v]);
+                } else if (row == 0) {
+                  out[v] = pred;
+                }
               } else {
-                if (row == 0) out[v] = pred[v];
+                gout = d.gvis[v];
               }
+              if (p.do_grid) gvring[gs * 4 + v] = gout;
             }
-          } else {
-#pragma unroll
-            for (int v = 0; v < N; ++v) gout[v] = d.gvis[v];
+            if (live && lane == 0 && p.do_grid) wchunk += d.twgt[row];
+            __syncwarp();
+            if (live && lane == 0) {
+              if (p.do_grid) ptx::mbar_arrive(&gvfull[gs]);
+              ptx::mbar_arrive(&empty[prev_s]);
+            }
+            __syncwarp();
+            TT_END(5);
           }
-          if (p.do_grid) {
-#pragma unroll
-            for (int v = 0; v < N; ++v) bcast[xs * 4 + v] = gout[v];
-            wchunk += d.twgt[row];
+          if (k < ch.count) {
+            prev_s = s;
+            ++q;
           }
         }
-        ptx::named_sync(1, kConsumers);
-        prev_s = s;
+      } else {
+        // -------- gridding warps --------
+        const int gw = warp - kGRBase;
+        for (int k = 0; k < ch.count; ++k, ++q) {
+          const int s = int(q % uint32_t(kSlots));
+          TT_BEGIN();
+          ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
+          TT_END(1);
+          if (p.do_grid) {
+            const int gs = int(q % uint32_t(kSlots));
+            TT_BEGIN();
+            ok &= ptx::mbar_wait(&gvfull[gs], (q / kSlots) & 1, abort);
+            TT_END(6);
+            TT_BEGIN();
+            if (!ptx::warp_flag(abort))
+            grid_rows<N, MIXED>(
+                p, descs[s],
+                reinterpret_cast<const float2*>(ring + ring_off[s]),
+                row, &gvring[gs * 4], gtile, gw, lane);
+            TT_END(7);
+          }
+          __syncwarp();
+          if (lane == 0) ptx::mbar_arrive(&empty[s]);
+        }
       }
-      if (prev_s >= 0) {
-        if (p.do_grid)
-          grid_cells<N, MIXED>(p, descs[prev_s],
-                               reinterpret_cast<const float2*>(
-                                   ring + size_t(prev_s) * p.slot_bytes),
-                               row, &bcast[((q - 1) & 1) * 4], gtile, ctid);
-        __syncwarp();
-        if (lane == 0) ptx::mbar_arrive(&empty[prev_s]);
-      }
+      TT_BEGIN();
       ptx::named_sync(1, kConsumers);
-      if (p.do_grid) {
+      if (p.do_grid && !*abort) {
         double2* plane = p.grid + size_t(cube * p.nrow + row) * p.ny * p.nx;
-        for (int i = ctid; i < RR; i += kConsumers) {
+        for (int i = tid; i < RR; i += kConsumers) {
           const int gx = x0 + i % p.R, gy = y0 + i / p.R;
           if (gx < p.nx && gy < p.ny) {
             const GT v = gtile[i];
@@ -676,9 +874,21 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             }
           }
         }
-        if (ctid == 0 && p.update_weights && ch.count > 0)
+        if (warp == kXWarp && lane == 0 && p.update_weights && ch.count > 0)
           atomicAdd(p.weights + size_t(cube) * p.nrow + row, wchunk);
       }
+      TT_END(8);
+    }
+    // timer slots: degridding warp 0 -> 0..3, exchange warp -> 4..6,
+    // first gridding warp -> 7..9
+    if (lane == 0 && warp == 0) {
+      TT_PUT(0, 0); TT_PUT(1, 1); TT_PUT(2, 2); TT_PUT(3, 8);
+    }
+    if (lane == 0 && warp == kXWarp) {
+      TT_PUT(4, 1); TT_PUT(5, 4); TT_PUT(6, 5); TT_PUT(10, 2); TT_PUT(11, 3);
+    }
+    if (lane == 0 && warp == kGRBase) {
+      TT_PUT(7, 1); TT_PUT(8, 6); TT_PUT(9, 7);
     }
   }
   if (!ok) atomicOr(p.status, kStatusWaitTimeout);
@@ -688,6 +898,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
 
 // ---------------------------------------------------------------------------
 // host side
+
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -705,7 +916,7 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 struct Plan {
   bool ok = false;
   std::string why;
-  int R = 0, T = 0, D = 0, slot_bytes = 0, K = 0;
+  int R = 0, T = 0, ring_bytes = 0, K = 0;
   TiledParams p{};
   int smem = 0;
 };
@@ -781,25 +992,27 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed) {
   const int eg = do_grid ? esize : 0;
   const int budget = 227 * 1024;
   const int taps = std::max(cf.max_taps_x, cf.max_taps_y);
-  for (int D = kMaxSlots; D >= 2; --D) {
-    const SmemLayout L0 = smem_layout(D, part, 0, em, eg);
+  // CF byte ring: about four of the largest parts (more in flight when
+  // parts are smaller), at least two; the tiles take the rest
+  for (int m = 4; m >= 2; --m) {
+    const int rb = m * part;
+    const SmemLayout L0 = smem_layout(rb, 0, em, eg);
     const int left = budget - L0.total - 1024 - 1024;
     if (left <= 0) continue;
     int R = (em + eg) > 0 ? int(std::sqrt(double(left) / double(em + eg))) : 128;
     R = std::min(R, 128) & ~1;
     if (R - taps + 1 < 4) continue;
-    pl.D = D;
+    pl.ring_bytes = rb;
     pl.R = R;
     break;
   }
-  if (pl.D == 0) {
+  if (pl.ring_bytes == 0) {
     pl.why = "CF slice part too large for the shared-memory ring";
     return pl;
   }
-  pl.slot_bytes = part;
   pl.T = pl.R - taps + 1;
   pl.K = mixed ? kChunkVisMixed : kChunkVisFP64;
-  pl.smem = smem_layout(pl.D, part, pl.R, em, eg).total + 1024;
+  pl.smem = smem_layout(pl.ring_bytes, pl.R, em, eg).total + 1024;
   if (em > 0 && (2 * size_t(g->grid_size[0]) * (mixed ? 4 : 8)) % 16 != 0) {
     pl.why = "model row pitch not a 16-byte multiple";
     return pl;
@@ -812,8 +1025,7 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed) {
   p.T = pl.T;
   p.ntx = (p.nx + pl.T - 1) / pl.T;
   p.nty = (p.ny + pl.T - 1) / pl.T;
-  p.D = pl.D;
-  p.slot_bytes = part;
+  p.ring_bytes = pl.ring_bytes;
   p.model_bytes = pl.R * pl.R * esize;
   p.esize_model = em;
   p.esize_grid = eg;
@@ -833,7 +1045,7 @@ Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
   // the kernel places its tiles with these sizes; they must match the form
   if ((p.esize_model != 0 && p.esize_model != int(sizeof(MT))) ||
       (p.esize_grid != 0 && p.esize_grid != int(sizeof(GT))) ||
-      smem_layout(p.D, p.slot_bytes, p.R, p.esize_model, p.esize_grid).total +
+      smem_layout(p.ring_bytes, p.R, p.esize_model, p.esize_grid).total +
               1024 > smem)
     return Status::err(HPGB_ERROR_OTHER, "tiled kernel layout mismatch");
   if ((p.do_degrid && p.has_model && p.esize_model == 0) ||
@@ -850,7 +1062,7 @@ Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cfg.blockDim = dim3(kThreadsTiled);
+  cfg.blockDim = dim3(kThreadsTiled);  // 18 warps
   cfg.dynamicSmemBytes = size_t(smem);
   cfg.stream = g->stream;
   int sms = 0;
@@ -952,6 +1164,15 @@ Status grid_tiled_n(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
   p.records = static_cast<unsigned char*>(d_vis);
   p.rec_stride = int(sizeof(VisData<N>));
   p.status = vb.counters.as<unsigned>();
+  p.timers = nullptr;
+#ifdef HPGB_TILED_TIMERS
+  {
+    static DevBuf timer_buf;
+    HPGB_TRY(timer_buf.reserve(148 * 16 * 8));
+    p.timers = timer_buf.as<unsigned long long>();
+    g_tiled_timers = p.timers;
+  }
+#endif
 
   CUtensorMap map;
   std::memset(&map, 0, sizeof(map));
@@ -1019,3 +1240,15 @@ Status grid_tiled(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
 }
 
 }  // namespace hpgb
+
+#ifdef HPGB_TILED_TIMERS
+// measurement builds only: copy out and clear the phase counters
+extern "C" __attribute__((visibility("default"))) int hpgb_debug_tiled_timers(
+    unsigned long long* out, int n) {
+  if (!hpgb::g_tiled_timers) return 1;
+  cudaDeviceSynchronize();
+  cudaMemcpy(out, hpgb::g_tiled_timers, size_t(n) * 8, cudaMemcpyDeviceToHost);
+  cudaMemset(hpgb::g_tiled_timers, 0, 148 * 16 * 8);
+  return 0;
+}
+#endif

@@ -7,6 +7,10 @@
 #include <cuda.h>
 #include <stdint.h>
 
+#ifndef WAIT_MAX_SLEEP_NS
+#define WAIT_MAX_SLEEP_NS 256
+#endif
+
 namespace hpgb {
 namespace ptx {
 
@@ -51,40 +55,77 @@ __device__ __forceinline__ void mbar_arrive_remote(uint64_t* bar,
       : "memory");
 }
 
-// Wait for the phase with the given parity to complete; gives up after
-// max_tries polls and returns false (the caller records the timeout).
+// Waits for the completion of the mbarrier phase with the given parity.
+// Every lane of the calling warp polls (try_wait), so the warp stays
+// converged; between polls the warp backs off with __nanosleep (doubling up
+// to kMaxSleepNs) so that waiting warps leave issue slots to working ones.
+// After kMaxTries polls (under a second) the wait gives up and returns
+// false, and the caller records the timeout instead of hanging.
+constexpr uint32_t kMaxTries = 1u << 21;
+constexpr uint32_t kMaxSleepNs = WAIT_MAX_SLEEP_NS;
+
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+      "selp.u32 %0, 1, 0, p; }"
+      : "=r"(done)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ bool mbar_try_cluster(uint32_t a, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.acquire.cluster.shared::cta."
+      "b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(done)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// `abort` is a CTA-wide shared-memory flag: a wait that gives up sets it,
+// and every later wait returns false at once, so a broken pipeline ends
+// quickly with an error status instead of timing out wait after wait.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
-                                          uint32_t max_tries = 1u << 24) {
+                                          volatile int* abort) {
   const uint32_t a = smem(bar);
-  for (uint32_t i = 0; i < max_tries; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], "
-        "%2; selp.u32 %0, 1, 0, p; }"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
+  uint32_t ns = 16;
+  for (uint32_t i = 0; i < kMaxTries; ++i) {
+    if (mbar_try(a, parity)) return true;
+    if (*abort) return false;
+    if (kMaxSleepNs) {
+      __nanosleep(ns);
+      ns = ns < kMaxSleepNs ? ns * 2 : kMaxSleepNs;
+    }
   }
+  *abort = 1;
   return false;
 }
 
-// same, with acquire at cluster scope (for barriers that remote CTAs arrive on)
+// acquire at cluster scope, for barriers that remote CTAs complete
 __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar,
                                                   uint32_t parity,
-                                                  uint32_t max_tries = 1u << 24) {
+                                                  volatile int* abort) {
   const uint32_t a = smem(bar);
-  for (uint32_t i = 0; i < max_tries; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.acquire.cluster.shared::cta."
-        "b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
+  uint32_t ns = 16;
+  for (uint32_t i = 0; i < kMaxTries; ++i) {
+    if (mbar_try_cluster(a, parity)) return true;
+    if (*abort) return false;
+    if (kMaxSleepNs) {
+      __nanosleep(ns);
+      ns = ns < kMaxSleepNs ? ns * 2 : kMaxSleepNs;
+    }
   }
+  *abort = 1;
   return false;
+}
+
+// warp-uniform read of a shared-memory flag (lane 0's view)
+__device__ __forceinline__ bool warp_flag(volatile int* flag) {
+  return __shfl_sync(0xffffffffu, *flag, 0) != 0;
 }
 
 // bulk copy global -> this CTA's shared memory, completion counted in bytes
@@ -126,6 +167,24 @@ __device__ __forceinline__ void st_cluster_f64(double* p, uint32_t rank,
                : "r"(smem(p)), "r"(rank));
   asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(remote), "d"(v)
                : "memory");
+}
+
+// asynchronous store of a double into CTA `rank`'s shared memory; its
+// completion is counted (8 bytes) on the mbarrier at bar's offset in that CTA
+__device__ __forceinline__ void st_async_f64(double* p, uint32_t rank, double v,
+                                             uint64_t* bar) {
+  uint32_t rp, rb;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+               : "=r"(rp)
+               : "r"(smem(p)), "r"(rank));
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+               : "=r"(rb)
+               : "r"(smem(bar)), "r"(rank));
+  asm volatile(
+      "st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, "
+      "[%2];" ::"r"(rp),
+      "d"(v), "r"(rb)
+      : "memory");
 }
 
 __device__ __forceinline__ uint32_t cluster_rank() {
