@@ -68,14 +68,16 @@ unsigned long long* g_tiled_timers = nullptr;
 
 namespace {
 
-// warp roles of the tiled kernel: kDG degridding warps, one exchange warp,
-// kGR gridding warps, one producer warp
+// warp roles of the tiled kernel: kDG degridding warps, kX exchange warps
+// (alternating visibilities), kGR gridding warps, one producer warp
 constexpr int kDG = 8;
+constexpr int kX = 2;
 constexpr int kGR = 8;
-constexpr int kXWarp = kDG;
-constexpr int kGRBase = kDG + 1;
+constexpr int kXBase = kDG;
+constexpr int kGRBase = kXBase + kX;
 constexpr int kPWarp = kGRBase + kGR;
-constexpr int kConsumers = (kDG + 1 + kGR) * 32;
+constexpr int kXSlots = 8;  // exchange buffers (visibility q uses q % 8)
+constexpr int kConsumers = (kDG + kX + kGR) * 32;
 constexpr int kThreadsTiled = kConsumers + 32;
 constexpr int kSlots = 8;  // descriptor slots (visibilities in flight)
 constexpr int kChunkVisFP64 = 2048;
@@ -165,11 +167,11 @@ __host__ __device__ inline SmemLayout smem_layout(int ring_bytes, int R,
                                                   int esize_model,
                                                   int esize_grid) {
   SmemLayout L;
-  // 33 mbarriers: full[8] empty[8] model xchg[4] dgfull[2] dgempty[2]
+  // 37 mbarriers: full[8] empty[8] model xchg[8] dgfull[2] dgempty[2]
   // gvfull[8], then the abort flag
   L.bars = 0;
-  L.xbuf = 320;                       // [4][4 rows][4 pol] complex double
-  L.wred = L.xbuf + 4 * 4 * 4 * 16;   // [2][kDG][8] double (degrid partials)
+  L.xbuf = 320;                       // [8][4 rows][4 pol] complex double
+  L.wred = L.xbuf + kXSlots * 4 * 4 * 16;  // [2][kDG][8] double (degrid partials)
   L.bcast = L.wred + 2 * kDG * 8 * 8; // [kSlots][4] float2 (gridding values)
   L.slots = L.bcast + kSlots * 4 * 8;  // ring_off[kSlots] int, slot_end[kSlots] u64
   L.desc = align_up(L.slots + kSlots * 4 + kSlots * 8, 128);
@@ -341,31 +343,50 @@ struct Form<true> {
   using grid_t = float2;
 };
 
-// Partial degridding sums of row `row` over the cells c = first, first +
-// stride, ... of one visibility's footprint (src/hpg_core.hpp:642-668).
+// Per-visibility values the cell loops need, copied out of the descriptor
+// into registers once per visibility.
+struct VisGeom {
+  int cx, cy, tx, ty, pst;
+  bool pos_w, screen_on;
+  double phi0x, phi0y, dphix, dphiy;
+};
+
+__device__ __forceinline__ VisGeom vis_geom(const TileDesc& d) {
+  VisGeom v;
+  v.cx = d.cx;
+  v.cy = d.cy;
+  v.tx = d.taps_x;
+  v.ty = d.taps_y;
+  v.pst = d.pstride;
+  v.pos_w = d.flags & kPosW;
+  v.screen_on = d.flags & kScreen;
+  v.phi0x = d.phi0[0];
+  v.phi0y = d.phi0[1];
+  v.dphix = d.dphi[0];
+  v.dphiy = d.dphi[1];
+  return v;
+}
+
+// Partial degridding sums of this CTA's row over the footprint cells
+// c = first, first + stride, ... of one visibility (src/hpg_core.hpp:642-668).
+// pp[v]: slot plane of Mueller element dmi[row][v] (-1 if inactive).
 template <int N, bool MIXED>
 __device__ __forceinline__ void degrid_cells(
-    const TiledParams& p, const TileDesc& d, const float2* cfs, int row,
-    const typename Form<MIXED>::model_t* mtile, int first, int stride,
-    double (&acc)[2 * N]) {
-  const bool pos_w = d.flags & kPosW;
-  const bool screen_on = d.flags & kScreen;
-  const int tx = d.taps_x, ncell = int(d.taps_x) * d.taps_y;
-  const int pst = d.pstride, R = p.R;
-  const float im = pos_w ? 1.0f : -1.0f;
-  int pp[N];
-#pragma unroll
-  for (int v = 0; v < N; ++v) pp[v] = p.dpos[row][pos_w ? 1 : 0][v];
+    const VisGeom& g, const int (&pp)[N], const float2* __restrict__ cfs,
+    const typename Form<MIXED>::model_t* __restrict__ mtile, int R, int first,
+    int stride, double (&acc)[2 * N]) {
+  const int tx = g.tx, ncell = g.tx * g.ty, pst = g.pst;
+  const float im = g.pos_w ? 1.0f : -1.0f;
   // (X, Y) of cell `first`, advanced incrementally
   int Y = first / tx, X = first - Y * tx;
   const int dY = stride / tx, dX = stride - dY * tx;
-  const typename Form<MIXED>::model_t* mrow = mtile + d.cy * R + d.cx;
+  const typename Form<MIXED>::model_t* mrow = mtile + g.cy * R + g.cx;
   if constexpr (!MIXED) {
     for (int c = first; c < ncell; c += stride) {
       double2 mv = mrow[Y * R + X];
-      if (screen_on) {
-        const double phx = __dadd_rn(d.phi0[0], __dmul_rn(double(X), d.dphi[0]));
-        const double phy = __dadd_rn(d.phi0[1], __dmul_rn(double(Y), d.dphi[1]));
+      if (g.screen_on) {
+        const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(X), g.dphix));
+        const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(Y), g.dphiy));
         mv = cmul_d(mv, cphase_d(__dsub_rn(-phx, phy)));
       }
 #pragma unroll
@@ -390,11 +411,11 @@ __device__ __forceinline__ void degrid_cells(
     for (int k = 0; k < 2 * N; ++k) a[k] = 0.f;
     for (int c = first; c < ncell; c += stride) {
       float2 mv = mrow[Y * R + X];
-      if (screen_on) {
-        const double phx = __dadd_rn(d.phi0[0], __dmul_rn(double(X), d.dphi[0]));
-        const double phy = __dadd_rn(d.phi0[1], __dmul_rn(double(Y), d.dphi[1]));
-        const double2 s = cphase_d(__dsub_rn(-phx, phy));
-        const float sx = float(s.x), sy = float(s.y);
+      if (g.screen_on) {
+        const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(X), g.dphix));
+        const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(Y), g.dphiy));
+        const double2 sc = cphase_d(__dsub_rn(-phx, phy));
+        const float sx = float(sc.x), sy = float(sc.y);
         mv = make_float2(mv.x * sx - mv.y * sy, mv.x * sy + mv.y * sx);
       }
 #pragma unroll
@@ -421,41 +442,31 @@ __device__ __forceinline__ void degrid_cells(
 // Gridding of one visibility into the rows of the grid tile owned by warp
 // `gw` (tile rows congruent to gw modulo kGR), so that different warps never
 // write the same tile cell (src/hpg_core.hpp:856-873).
+// pp[v]: slot plane of Mueller element gmi[row][v] (-1 if inactive).
 template <int N, bool MIXED>
-__device__ __forceinline__ void grid_rows(const TiledParams& p,
-                                          const TileDesc& d, const float2* cfs,
-                                          int row, const float2* gvis,
-                                          typename Form<MIXED>::grid_t* gtile,
-                                          int gw, int lane) {
-  const bool pos_w = d.flags & kPosW;
-  const bool screen_on = d.flags & kScreen;
-  const int tx = d.taps_x, ty = d.taps_y;
-  const int pst = d.pstride, R = p.R;
-  const float im = pos_w ? -1.0f : 1.0f;
-  const int Y0 = (gw - d.cy % kGR + kGR) % kGR;  // first footprint row owned
+__device__ __forceinline__ void grid_rows(
+    const VisGeom& g, const int (&pp)[N], const float2* __restrict__ cfs,
+    const float2 (&gv)[N], typename Form<MIXED>::grid_t* __restrict__ gtile,
+    int R, int gw, int lane) {
+  const int tx = g.tx, ty = g.ty, pst = g.pst;
+  const float im = g.pos_w ? -1.0f : 1.0f;
+  const int Y0 = (gw - g.cy % kGR + kGR) % kGR;  // first footprint row owned
   if (Y0 >= ty) return;
   const int nr = (ty - Y0 + kGR - 1) / kGR;
   const int ncw = nr * tx;  // cells of this warp
-  int pp[N];
-  float2 gv[N];
-#pragma unroll
-  for (int v = 0; v < N; ++v) {
-    pp[v] = p.gpos[row][pos_w ? 1 : 0][v];
-    gv[v] = gvis[v];
-  }
   // flattened index i -> (row r_i, X); footprint row Y = Y0 + r_i*kGR
   int ri = lane / tx, X = lane - ri * tx;
   const int dR = 32 / tx, dX = 32 - dR * tx;
-  typename Form<MIXED>::grid_t* gbase = gtile + d.cy * R + d.cx;
+  typename Form<MIXED>::grid_t* gbase = gtile + g.cy * R + g.cx;
   for (int i = lane; i < ncw; i += 32) {
     const int Y = Y0 + ri * kGR;
     const int c = Y * tx + X;
     float2 screen = make_float2(1.0f, 0.0f);
-    if (screen_on) {
-      const double phx = __dadd_rn(d.phi0[0], __dmul_rn(double(X), d.dphi[0]));
-      const double phy = __dadd_rn(d.phi0[1], __dmul_rn(double(Y), d.dphi[1]));
-      const double2 s = cphase_d(__dadd_rn(phx, phy));
-      screen = make_float2(__double2float_rn(s.x), __double2float_rn(s.y));
+    if (g.screen_on) {
+      const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(X), g.dphix));
+      const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(Y), g.dphiy));
+      const double2 sc = cphase_d(__dadd_rn(phx, phy));
+      screen = make_float2(__double2float_rn(sc.x), __double2float_rn(sc.y));
     }
     const int idx = Y * R + X;
     if constexpr (!MIXED) {
@@ -465,8 +476,8 @@ __device__ __forceinline__ void grid_rows(const TiledParams& p,
         if (pp[v] >= 0) {
           float2 cf = cfs[pp[v] * pst + c];
           cf.y *= im;
-          const float2 prod =
-              screen_on ? cmul_f(cmul_f(cf, screen), gv[v]) : cmul_f(cf, gv[v]);
+          const float2 prod = g.screen_on ? cmul_f(cmul_f(cf, screen), gv[v])
+                                          : cmul_f(cf, gv[v]);
           sx = __dadd_rn(sx, double(prod.x));
           sy = __dadd_rn(sy, double(prod.y));
         }
@@ -482,7 +493,7 @@ __device__ __forceinline__ void grid_rows(const TiledParams& p,
         if (pp[v] >= 0) {
           float2 cf = cfs[pp[v] * pst + c];
           cf.y *= im;
-          if (screen_on)
+          if (g.screen_on)
             cf = make_float2(cf.x * screen.x - cf.y * screen.y,
                              cf.x * screen.y + cf.y * screen.x);
           sx = fmaf(cf.x, gv[v].x, fmaf(-cf.y, gv[v].y, sx));
@@ -519,12 +530,12 @@ tiled_kernel(const __grid_constant__ TiledParams p,
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + L.bars);
   uint64_t* empty = full + kSlots;
   uint64_t* model_bar = empty + kSlots;
-  uint64_t* xchg = model_bar + 1;  // [4]
-  uint64_t* dgfull = xchg + 4;     // [2]
+  uint64_t* xchg = model_bar + 1;  // [kXSlots]
+  uint64_t* dgfull = xchg + kXSlots;  // [2]
   uint64_t* dgempty = dgfull + 2;  // [2]
   uint64_t* gvfull = dgempty + 2;  // [kSlots]
   volatile int* abort = reinterpret_cast<volatile int*>(gvfull + kSlots);
-  double* xbuf = reinterpret_cast<double*>(sm + L.xbuf);  // [4][4][4][2]
+  double* xbuf = reinterpret_cast<double*>(sm + L.xbuf);  // [8][4][4][2]
   double* dgpart = reinterpret_cast<double*>(sm + L.wred);  // [2][kDG][8]
   // gridding values of visibility q in entry q % kSlots: the exchange warp
   // runs at most kSlots - 1 visibilities ahead of the gridding warps (the
@@ -543,7 +554,8 @@ tiled_kernel(const __grid_constant__ TiledParams p,
   const int row = int(ptx::cluster_rank());
   const unsigned cid = ptx::cluster_id_x(), ncl = ptx::num_clusters_x();
   const bool exchange = p.do_degrid && p.has_model;
-  // every role that reads a ring slot releases it
+  // every role that reads a ring slot releases it (one exchange warp per
+  // visibility)
   const uint32_t empty_count = uint32_t((exchange ? kDG : 0) + 1 + kGR);
 
   if (tid == 0) {
@@ -552,7 +564,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       ptx::mbar_init(&empty[s], empty_count);
     }
     ptx::mbar_init(model_bar, 1);
-    for (int x = 0; x < 4; ++x) ptx::mbar_init(&xchg[x], 1);
+    for (int x = 0; x < kXSlots; ++x) ptx::mbar_init(&xchg[x], 1);
     for (int x = 0; x < 2; ++x) {
       ptx::mbar_init(&dgfull[x], kDG);
       ptx::mbar_init(&dgempty[x], 1);
@@ -566,7 +578,18 @@ tiled_kernel(const __grid_constant__ TiledParams p,
 
   const unsigned nchunks = *p.num_chunks;
   bool ok = true;
-  const int RR = p.R * p.R;
+  const int R = p.R;
+  const int RR = R * R;
+  // slot planes of this row's Mueller elements for w <= 0 and w > 0, one
+  // signed byte per element (-1: inactive), packed four to a register
+  uint32_t dpk[2] = {0u, 0u}, gpk[2] = {0u, 0u};
+#pragma unroll
+  for (int w = 0; w < 2; ++w)
+#pragma unroll
+    for (int v = 0; v < N; ++v) {
+      dpk[w] |= uint32_t(p.dpos[row][w][v] & 0xff) << (8 * v);
+      gpk[w] |= uint32_t(p.gpos[row][w][v] & 0xff) << (8 * v);
+    }
 
   if (warp == kPWarp) {
     // ---------------- producer warp ----------------
@@ -579,6 +602,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
     uint32_t q = 0;
     uint32_t q_old = 0;               // oldest visibility not yet reclaimed
     unsigned long long head = 0;      // ring bytes allocated (monotonic)
+    uint32_t pos = 0;                 // head modulo the ring size
     unsigned long long tail = 0;      // ring bytes released (monotonic)
     TT_DECL(2);
     for (unsigned c = cid; c < nchunks; c += ncl) {
@@ -605,19 +629,21 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         // straddle the ring end; they are released in order).
         const bool cf_needed = exchange || p.do_grid;
         const uint32_t pbytes = uint32_t(pstride) * 8u;
-        const unsigned long long need =
-            cf_needed ? (unsigned long long)(p.nplanes[row]) * pbytes : 0ull;
+        const uint32_t need = cf_needed ? uint32_t(p.nplanes[row]) * pbytes : 0u;
+        const uint32_t rb = uint32_t(p.ring_bytes);
         TT_BEGIN();
         for (;;) {
           unsigned long long h = head;
-          const unsigned long long pos = h % (unsigned long long)p.ring_bytes;
-          if (need > 0 && pos + need > (unsigned long long)p.ring_bytes)
-            h += (unsigned long long)p.ring_bytes - pos;
+          uint32_t ps = pos;
+          if (need > 0 && ps + need > rb) {
+            h += rb - ps;
+            ps = 0;
+          }
           const bool need_slot = (q - q_old) >= uint32_t(kSlots);
-          const bool need_space =
-              need > 0 && h + need - tail > (unsigned long long)p.ring_bytes;
+          const bool need_space = need > 0 && h + need - tail > rb;
           if (!need_slot && !need_space) {
             head = h;
+            pos = ps;
             break;
           }
           if (q_old == q) {  // cannot happen: the plan keeps need <= ring
@@ -634,10 +660,10 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         // after an abort nothing is copied into slots that may still be read
         if (lane == 0 && !*abort) {
           TT_BEGIN();
-          const int roff = int(head % (unsigned long long)p.ring_bytes);
+          const int roff = int(pos);
           ring_off[s] = roff;
           slot_end[s] = head + need;
-          ptx::mbar_expect_tx(&full[s], uint32_t(sizeof(TileDesc)) + uint32_t(need));
+          ptx::mbar_expect_tx(&full[s], uint32_t(sizeof(TileDesc)) + need);
           ptx::bulk_g2s(&descs[s], &p.descs[ch.start + k],
                         uint32_t(sizeof(TileDesc)), &full[s]);
           if (cf_needed) {
@@ -658,14 +684,15 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           TT_END(1);
         }
         head += need;
+        pos += need;
         __syncwarp();
       }
     }
     if (lane == 0) { TT_STORE(blockIdx.x * 16 + 12, 2); }
   } else {
     // ---------------- consumer roles ----------------
-    // degridding warps [0, kDG), exchange warp kXWarp, gridding warps
-    // [kGRBase, kGRBase + kGR).  Roles hand visibilities to each other
+    // degridding warps [0, kDG), exchange warps [kXBase, kGRBase), gridding
+    // warps [kGRBase, kGRBase + kGR).  Roles hand visibilities to each other
     // through mbarriers; all of them meet at chunk boundaries.
     uint32_t q = 0;
     uint32_t model_phase = 0;
@@ -714,46 +741,84 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           double acc[2 * N];
 #pragma unroll
           for (int t = 0; t < 2 * N; ++t) acc[t] = 0.0;
-          degrid_cells<N, MIXED>(
-              p, descs[s],
-              reinterpret_cast<const float2*>(ring + ring_off[s]),
-              row, mtile, warp * 32 + lane, kDG * 32, acc);
+          {
+            const VisGeom vg = vis_geom(descs[s]);
+            int pp[N];
 #pragma unroll
-          for (int t = 0; t < 2 * N; ++t) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-              acc[t] += __shfl_down_sync(0xffffffffu, acc[t], o);
+            for (int v = 0; v < N; ++v)
+              pp[v] = int(int8_t((vg.pos_w ? dpk[1] : dpk[0]) >> (8 * v)));
+            degrid_cells<N, MIXED>(
+                vg, pp, reinterpret_cast<const float2*>(ring + ring_off[s]),
+                mtile, R, warp * 32 + lane, kDG * 32, acc);
           }
+          // warp sum of the 8 (padded) partials: halve the values held per
+          // lane at each of the first three levels, then butterfly; lane
+          // L ends with the sum of value ((L>>4)&1)*4 + ((L>>3)&1)*2 + ((L>>2)&1)
+          double v8[8];
+#pragma unroll
+          for (int t = 0; t < 8; ++t) v8[t] = t < 2 * N ? acc[t] : 0.0;
+          double v4[4], v2[2], v1;
+          {
+            const bool hi = lane & 16;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              const double give = hi ? v8[i] : v8[i + 4];
+              const double keep = hi ? v8[i + 4] : v8[i];
+              v4[i] = keep + __shfl_xor_sync(0xffffffffu, give, 16);
+            }
+          }
+          {
+            const bool hi = lane & 8;
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              const double give = hi ? v4[i] : v4[i + 2];
+              const double keep = hi ? v4[i + 2] : v4[i];
+              v2[i] = keep + __shfl_xor_sync(0xffffffffu, give, 8);
+            }
+          }
+          {
+            const bool hi = lane & 4;
+            const double give = hi ? v2[0] : v2[1];
+            const double keep = hi ? v2[1] : v2[0];
+            v1 = keep + __shfl_xor_sync(0xffffffffu, give, 4);
+          }
+          v1 += __shfl_xor_sync(0xffffffffu, v1, 2);
+          v1 += __shfl_xor_sync(0xffffffffu, v1, 1);
+          const int vidx = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 +
+                           ((lane >> 2) & 1);
           TT_END(2);
           const int b = int(q & 1);
           if (q >= 2) ok &= ptx::mbar_wait(&dgempty[b], ((q >> 1) & 1) ^ 1, abort);
           if (ptx::warp_flag(abort)) continue;
+          if ((lane & 3) == 0) dgpart[(b * kDG + warp) * 8 + vidx] = v1;
+          __syncwarp();
           if (lane == 0) {
-#pragma unroll
-            for (int t = 0; t < 2 * N; ++t) dgpart[(b * kDG + warp) * 8 + t] = acc[t];
             ptx::mbar_arrive(&dgfull[b]);
             ptx::mbar_arrive(&empty[s]);
           }
           __syncwarp();
         }
-      } else if (warp == kXWarp) {
-        // -------- exchange warp --------
-        // Step k sends the row partials of visibility q (k < count) and then
-        // finishes visibility q-1, whose partials from the other rows were
-        // sent one step earlier and have normally arrived by now.
+      } else if (warp < kGRBase) {
+        // -------- exchange warps --------
+        // Exchange warp xw takes the visibilities q with q % 2 == xw (the
+        // degrid partial buffer q % 2 is its own).  For each of them it
+        // sends this row's partials to every CTA of the cluster, then
+        // finishes its previous visibility, whose partials from the other
+        // rows were sent one step earlier and have normally arrived.
+        const int xw = warp - kXBase;
         int prev_s = -1;
+        uint32_t prev_q = 0;
         for (int k = 0; k <= ch.count; ++k) {
+          const bool mine = k < ch.count && (q & 1) == uint32_t(xw);
           int s = -1;
-          if (k < ch.count) {
+          if (mine) {
             s = int(q % uint32_t(kSlots));
             TT_BEGIN();
             ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
             TT_END(1);
             if (exchange && !ptx::warp_flag(abort)) {
-              TT_BEGIN();
-              const int xs = int(q & 3);
-              const int b = int(q & 1);
-              TT_END(4);
+              const int xs = int(q % uint32_t(kXSlots));
+              const int b = xw;
               TT_BEGIN();
               ok &= ptx::mbar_wait(&dgfull[b], (q >> 1) & 1, abort);
               TT_END(2);
@@ -777,15 +842,14 @@ tiled_kernel(const __grid_constant__ TiledParams p,
               TT_END(4);
             }
           }
-          if (prev_s >= 0) {
+          if ((mine || k == ch.count) && prev_s >= 0) {
             TT_BEGIN();
-            const uint32_t qq = q - 1;
+            const uint32_t qq = prev_q;
             const TileDesc& d = descs[prev_s];
-            const int xs = int(qq & 3);
+            const int xs = int(qq % uint32_t(kXSlots));
             const int gs = int(qq % uint32_t(kSlots));
-            TT_END(5);
-            TT_BEGIN();
-            if (exchange) ok &= ptx::mbar_wait_cluster(&xchg[xs], (qq >> 2) & 1, abort);
+            if (exchange)
+              ok &= ptx::mbar_wait_cluster(&xchg[xs], (qq / kXSlots) & 1, abort);
             TT_END(3);
             TT_BEGIN();
             const bool live = !ptx::warp_flag(abort);
@@ -827,12 +891,14 @@ tiled_kernel(const __grid_constant__ TiledParams p,
               ptx::mbar_arrive(&empty[prev_s]);
             }
             __syncwarp();
+            prev_s = -1;
             TT_END(5);
           }
-          if (k < ch.count) {
+          if (mine) {
             prev_s = s;
-            ++q;
+            prev_q = q;
           }
+          if (k < ch.count) ++q;
         }
       } else {
         // -------- gridding warps --------
@@ -848,11 +914,19 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             ok &= ptx::mbar_wait(&gvfull[gs], (q / kSlots) & 1, abort);
             TT_END(6);
             TT_BEGIN();
-            if (!ptx::warp_flag(abort))
-            grid_rows<N, MIXED>(
-                p, descs[s],
-                reinterpret_cast<const float2*>(ring + ring_off[s]),
-                row, &gvring[gs * 4], gtile, gw, lane);
+            if (!ptx::warp_flag(abort)) {
+              const VisGeom vg = vis_geom(descs[s]);
+              int pp[N];
+              float2 gv[N];
+#pragma unroll
+              for (int v = 0; v < N; ++v) {
+                pp[v] = int(int8_t((vg.pos_w ? gpk[1] : gpk[0]) >> (8 * v)));
+                gv[v] = gvring[gs * 4 + v];
+              }
+              grid_rows<N, MIXED>(
+                  vg, pp, reinterpret_cast<const float2*>(ring + ring_off[s]),
+                  gv, gtile, R, gw, lane);
+            }
             TT_END(7);
           }
           __syncwarp();
@@ -864,7 +938,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       if (p.do_grid && !*abort) {
         double2* plane = p.grid + size_t(cube * p.nrow + row) * p.ny * p.nx;
         for (int i = tid; i < RR; i += kConsumers) {
-          const int gx = x0 + i % p.R, gy = y0 + i / p.R;
+          const int gx = x0 + i % R, gy = y0 + i / R;
           if (gx < p.nx && gy < p.ny) {
             const GT v = gtile[i];
             if (v.x != 0 || v.y != 0) {
@@ -874,7 +948,8 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             }
           }
         }
-        if (warp == kXWarp && lane == 0 && p.update_weights && ch.count > 0)
+        if (warp >= kXBase && warp < kGRBase && lane == 0 && p.update_weights &&
+            wchunk != 0.0)
           atomicAdd(p.weights + size_t(cube) * p.nrow + row, wchunk);
       }
       TT_END(8);
@@ -884,7 +959,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
     if (lane == 0 && warp == 0) {
       TT_PUT(0, 0); TT_PUT(1, 1); TT_PUT(2, 2); TT_PUT(3, 8);
     }
-    if (lane == 0 && warp == kXWarp) {
+    if (lane == 0 && warp == kXBase) {
       TT_PUT(4, 1); TT_PUT(5, 4); TT_PUT(6, 5); TT_PUT(10, 2); TT_PUT(11, 3);
     }
     if (lane == 0 && warp == kGRBase) {
