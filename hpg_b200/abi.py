@@ -54,6 +54,9 @@ CF_LAYOUT_LOGICAL = 0
 CF_LAYOUT_CUDA_V0 = 1
 CF_LAYOUT_HOST_V0 = 2
 
+# capacity of the fixed scratch array of hpgb_grid_visibilities_noalloc
+NOALLOC_MAX_VALUES = 1048576
+
 
 class HpgError(RuntimeError):
     """A failed C-ABI call; ``type`` is the hpg::ErrorType name."""
@@ -111,6 +114,7 @@ SIGNATURES = {
     "hpgb_set_cf": ([_P, _U, _U, _P, _PP, _I, _I], _I),
     "hpgb_set_model": ([_P, _P, _P, _I, _I], _I),
     "hpgb_grid_visibilities": ([_P, _P, _S, _U, _U, _I, _P], _I),
+    "hpgb_grid_visibilities_noalloc": ([_P, _P, _S, _U, _U], _I),
     "hpgb_fence": ([_P], _I),
     "hpgb_copy_weights": ([_P, _P, _I], _I),
     "hpgb_copy_grid": ([_P, _P, _I], _I),

@@ -436,6 +436,31 @@ int hpgb_grid_visibilities(hpgb_gridder* g, const void* vis, size_t n,
   });
 }
 
+int hpgb_grid_visibilities_noalloc(hpgb_gridder* g, void* vis, size_t n,
+                                   unsigned npol, unsigned flags) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    // validation order of src/hpg_runtime.hpp:1816-1828
+    if (n > g->max_batch)
+      return Status::err(HPGB_ERROR_EXCESSIVE_NUMBER_VISIBILITIES,
+                         "Number of visibilities exceeds maximum batch size");
+    if (npol != g->npol)
+      return Status::err(HPGB_ERROR_INVALID_NUMBER_POLARIZATIONS,
+                         "Number of visibility polarizations does not match "
+                         "Mueller matrix");
+    if (!(flags & HPGB_DO_GRID) && (flags & HPGB_UPDATE_GRID_WEIGHTS))
+      return Status::err(HPGB_ERROR_UPDATE_WEIGHTS_WITHOUT_GRIDDING,
+                         "Unable to update grid weights during degridding only");
+    if (n == 0) return Status::ok();
+    if (!vis) return Status::err(HPGB_ERROR_OTHER, "null visibilities");
+    if (!g->cf.set)
+      return Status::err(HPGB_ERROR_OTHER, "no convolution function set");
+    HPGB_TRY(validate_mueller(g));
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    return grid_direct_noalloc(g, vis, n, flags);
+  });
+}
+
 int hpgb_fence(const hpgb_gridder* g) {
   return guarded([&]() -> Status {
     if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");

@@ -15,6 +15,9 @@
 // The normaliser sum_XY cf and the weight sums come from the per-slice FP64
 // sums computed when the CF is set (CFGroup::wsum).
 
+#include <mutex>
+#include <string>
+
 #include "gridder.cuh"
 
 namespace hpgb {
@@ -297,6 +300,101 @@ Status debug_coords(hpgb_gridder* g, const void* d_vis, size_t n,
   HPGB_CUDA_TRY(cudaGetLastError());
   ++g->launches;
   return Status::ok();
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free form of the direct path (hpgb_grid_visibilities_noalloc).
+//
+// Some callers cannot allocate device memory when they grid: cudaMalloc and
+// cudaFree can synchronize the whole device, which stalls every other stream
+// of a pipeline that overlaps gridding with transfers, and they fail outright
+// in a process that handed nearly all device memory to its own pool when it
+// started.  For them the only per-call scratch of the direct path, the
+// gridding values of each visibility (float2 [n][N]), lives in a fixed
+// device array compiled into this library instead of a gridder buffer.
+//
+// The array needs no initial value: the degridding kernel (or
+// gvis_init_kernel when only gridding) writes the entry of every visibility
+// that lies on the grid before grid_direct_kernel reads it in the same call,
+// and visibilities off the grid are skipped by both.  There is one array per
+// device, shared by every gridder: two calls that can run at the same time
+// on one device (different streams with no ordering between them) race on
+// it.
+
+namespace {
+
+__device__ __align__(256) float2 g_noalloc_gvis[kNoAllocMaxValues];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex noalloc_mtx;
+float2* noalloc_addr[kNoAllocMaxDevices] = {};
+
+// device address of g_noalloc_gvis on `device`, looked up once per device
+// with that device current
+Status noalloc_scratch(int device, float2** out) {
+  if (device < 0 || device >= kNoAllocMaxDevices)
+    return Status::err(HPGB_ERROR_OTHER, "device index out of range");
+  std::lock_guard<std::mutex> lock(noalloc_mtx);
+  if (!noalloc_addr[device]) {
+    void* p = nullptr;
+    HPGB_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_gvis));
+    noalloc_addr[device] = static_cast<float2*>(p);
+  }
+  *out = noalloc_addr[device];
+  return Status::ok();
+}
+
+template <int N>
+Status grid_direct_noalloc_n(hpgb_gridder* g, void* d_vis, size_t n,
+                             unsigned flags) {
+  if (n == 0) return Status::ok();
+  const bool do_grid = flags & HPGB_DO_GRID;
+  if (do_grid && n * N > kNoAllocMaxValues)
+    return Status::err(
+        HPGB_ERROR_EXCESSIVE_NUMBER_VISIBILITIES,
+        "allocation-free gridding holds at most " +
+            std::to_string(kNoAllocMaxValues) +
+            " visibility polarization values per call (" +
+            std::to_string(kNoAllocMaxValues / N) + " visibilities of " +
+            std::to_string(N) + " polarizations)");
+  float2* gvis = nullptr;
+  HPGB_TRY(noalloc_scratch(g->device, &gvis));
+  VisData<N>* vis = static_cast<VisData<N>*>(d_vis);
+  const GridGeom geom = g->geom();
+  const CFGroup* groups = g->cf.desc.as<const CFGroup>();
+  if (flags & HPGB_DO_DEGRID) {
+    degrid_direct_kernel<N><<<unsigned(n), kThreads, 0, g->stream>>>(
+        vis, n, geom, groups,
+        g->has_model ? g->model.as<const double2>() : nullptr, gvis, do_grid);
+    HPGB_CUDA_TRY(cudaGetLastError());
+    ++g->launches;
+  } else if (do_grid) {
+    gvis_init_kernel<N><<<unsigned((n + 255) / 256), 256, 0, g->stream>>>(
+        vis, n, gvis);
+    HPGB_CUDA_TRY(cudaGetLastError());
+    ++g->launches;
+  }
+  if (do_grid) {
+    grid_direct_kernel<N><<<unsigned(n), kThreads, 0, g->stream>>>(
+        vis, n, geom, groups, gvis, g->grid.as<double2>(),
+        (flags & HPGB_UPDATE_GRID_WEIGHTS) ? g->weights.as<double>() : nullptr);
+    HPGB_CUDA_TRY(cudaGetLastError());
+    ++g->launches;
+  }
+  return Status::ok();
+}
+
+}  // namespace
+
+Status grid_direct_noalloc(hpgb_gridder* g, void* d_vis, size_t n,
+                           unsigned flags) {
+  switch (g->npol) {
+    case 1: return grid_direct_noalloc_n<1>(g, d_vis, n, flags);
+    case 2: return grid_direct_noalloc_n<2>(g, d_vis, n, flags);
+    case 3: return grid_direct_noalloc_n<3>(g, d_vis, n, flags);
+    case 4: return grid_direct_noalloc_n<4>(g, d_vis, n, flags);
+    default: return Status::err(HPGB_ERROR_OTHER, "bad polarization count");
+  }
 }
 
 }  // namespace hpgb

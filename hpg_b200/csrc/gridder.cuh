@@ -109,6 +109,11 @@ Status grid_tiled(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
 // grid_direct.cu
 Status grid_direct(hpgb_gridder* g, const void* d_vis, size_t n,
                    unsigned flags);
+// direct path with its per-visibility scratch in a fixed device array of
+// kNoAllocMaxValues complex<float> values: allocates no device memory
+constexpr size_t kNoAllocMaxValues = HPGB_NOALLOC_MAX_VALUES;
+Status grid_direct_noalloc(hpgb_gridder* g, void* d_vis, size_t n,
+                           unsigned flags);
 Status debug_coords(hpgb_gridder* g, const void* d_vis, size_t n,
                     hpgb_vis_coords* d_out);
 

@@ -220,6 +220,38 @@ HPGB_API int hpgb_grid_visibilities(hpgb_gridder* gridder, const void* visibilit
                            size_t num_visibilities, unsigned num_polarizations,
                            unsigned flags, int vis_on_device, void* returned);
 
+/* Allocation-free degridding/gridding of device-resident visibilities.
+ * No counterpart in the reference's State: it serves callers that must not
+ * allocate device memory while they grid (cudaMalloc/cudaFree can
+ * synchronize the device, and fail in a process whose memory is already
+ * handed to its own pool).  It runs the direct kernels of
+ * hpgb_grid_visibilities (those of HPGB_KERNEL_DIRECT, FP64 arithmetic, for
+ * either precision setting) on the caller's records in place, with the one
+ * per-call scratch array, the gridding value of each visibility
+ * polarization, in a fixed device array of HPGB_NOALLOC_MAX_VALUES
+ * complex<float> values (8 MiB) compiled into the library.
+ *
+ * visibilities: num_visibilities hpgb_visdataN records in DEVICE memory.
+ * With HPGB_DO_DEGRID their vis values are overwritten in place (predicted
+ * values, residuals with HPGB_DO_GRID) and are valid after hpgb_fence();
+ * HPGB_RETURN_VISIBILITIES is not needed.  Validation as
+ * hpgb_grid_visibilities, then: gridding a batch of more than
+ * HPGB_NOALLOC_MAX_VALUES / num_polarizations visibilities returns
+ * ExcessiveNumberVisibilities and launches nothing.
+ * The scratch array needs no initial value (every entry read is written
+ * earlier in the same call).  There is one per device, shared by all
+ * gridders: calls that may run at the same time on one device (streams with
+ * no ordering between them) race on it; calls on one gridder are ordered by
+ * its stream.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture
+ * starts on the device. */
+#define HPGB_NOALLOC_MAX_VALUES 1048576u
+HPGB_API int hpgb_grid_visibilities_noalloc(hpgb_gridder* gridder,
+                                            void* visibilities,
+                                            size_t num_visibilities,
+                                            unsigned num_polarizations,
+                                            unsigned flags);
+
 /* State::fence (src/hpg_runtime.hpp:153-154). */
 HPGB_API int hpgb_fence(const hpgb_gridder* gridder);
 
