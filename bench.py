@@ -1,7 +1,7 @@
 """Benchmark of the gridding / degridding hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--precision mixed|fp64] [--nvis 10000000]
+                    [--precision both|mixed|fp64] [--nvis 10000000]
 
 Workload (one "step"): degrid_grid_visibilities of one batch of 10M
 four-polarization visibilities onto a 2048x2048x4x1 complex128 grid with a
@@ -9,11 +9,14 @@ dense 4x4 Mueller matrix (16 CF planes), 8 w-plane CF groups with supports
 8..32 (9..33 taps) at oversampling 128, starting from a complex128 N(0,1)
 model.  All inputs are seeded synthetic data with those shapes.
 
-Printed (rank 0, one JSON line): Mvis/s with inputs resident in HBM
-("value"), the same through the public API with pinned host input and a
-device->host read of the weights ("e2e"), the HBM roofline of the step, the
-CPU baseline (threaded CPU restatement on a bounded sample) and the SM clocks
-sampled during the timed region.
+Printed (rank 0, one JSON line): Mvis/s of the mixed form with inputs
+resident in HBM ("value"; the FP64 form is timed beside it under "forms"),
+the same through the public API with pinned host input and a device->host
+read of the weights ("e2e"), the HBM roofline of the tiled kernel (its
+algorithmic bytes over its CUDA-event time) and of the whole step, the error
+of the mixed grid against the FP64 grid at full size, the CPU baseline
+(threaded CPU restatement on a bounded sample) and the SM clocks sampled
+during the timed region.
 
 Under torchrun (N > 1) every rank runs its own replica of the workload on its
 GPU (weak scaling); the step time is the maximum over ranks.
@@ -42,7 +45,10 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--precision", default="fp64", choices=["mixed", "fp64"])
+    p.add_argument("--precision", default="both",
+                   choices=["both", "mixed", "fp64"],
+                   help="both: the mixed form is the headline, the FP64 form "
+                        "is timed beside it")
     p.add_argument("--nvis", type=int, default=10_000_000)
     p.add_argument("--grid", type=int, default=2048)
     p.add_argument("--oversampling", type=int, default=128,
@@ -142,6 +148,20 @@ def make_workload(args, seed_offset, device):
                     dtype=torch.float64))
     return dict(p=p, grid_size=grid_size, vis=vis, cf_extents=ext,
                 cf_values=vals, model=model)
+
+
+# DRAM bytes (read + write) of one tiled-kernel launch, from an ncu capture
+# of 200k visibilities of this workload at CF oversampling 64 (mixed form:
+# 17.19 GB, of which 0.67 GB are the model and grid passes), scaled to a
+# launch by the visibility count.
+TRAFFIC_PER_VIS_MIXED = (17.193e9 - 0.671e9) / 200_000
+TRAFFIC_PER_VIS_FP64 = (16.914e9 - 0.805e9) / 200_000
+
+
+def kernel_traffic(form, nvis, grid_elems):
+    if form == "mixed":
+        return TRAFFIC_PER_VIS_MIXED * nvis + grid_elems * (8 + 32)
+    return TRAFFIC_PER_VIS_FP64 * nvis + grid_elems * (16 + 32)
 
 
 def taps_of(supports):
@@ -253,8 +273,6 @@ def main():
     p = wl["p"]
     g = Gridder.create(local_rank, 0, args.nvis, None, wl["grid_size"],
                        p["grid_scale"], p["mueller"], p["conj_mueller"])
-    g.set_precision(hpg_b200.PRECISION_MIXED if args.precision == "mixed"
-                    else hpg_b200.PRECISION_FP64)
     g.set_convolution_function(CFArray(p["oversampling"], wl["cf_extents"],
                                        wl["cf_values"]), on_device=True)
     g.set_model(wl["model"], on_device=True)
@@ -278,10 +296,6 @@ def main():
         g.degrid_grid_visibilities(hvis_np)
         return g.grid_weights()
 
-    for _ in range(args.warmup):
-        step_device()
-    g.fence()
-
     def timed(fn, k):
         if world > 1:
             dist.barrier()
@@ -304,30 +318,80 @@ def main():
             dist.barrier()
         return ms
 
-    clocks = ClockSampler(local_rank)
-    clocks.start()
-    launches0 = g.kernel_launches()
-    ms = timed(step_device, args.steps)
-    launches = g.kernel_launches() - launches0
-    clock_summary = clocks.stop()
+    taps = taps_of(p["supports"])
+    grid_elems = int(np.prod(wl["grid_size"]))
+    b_alg = workloads.algorithmic_bytes(vis, 4, taps, 16, grid_elems, 3)
+    # the tiled kernel's share: CF slices + model read + grid read/write (the
+    # visibility records are read by the sort and descriptor kernels)
+    b_kernel = b_alg - len(vis) * vis.dtype.itemsize
+    peak, peak_kind = peaks()
+    total_vis = args.nvis * world
 
-    e2e_steps = max(1, min(args.steps, 3))
-    ms_e2e = None
+    forms = (["mixed", "fp64"] if args.precision == "both"
+             else [args.precision])
+    results = {}
+    clock_summary = None
+    for form in forms:
+        g.set_precision(hpg_b200.PRECISION_MIXED if form == "mixed"
+                        else hpg_b200.PRECISION_FP64)
+        for _ in range(args.warmup):
+            step_device()
+        g.fence()
+        g.tiled_kernel_time()
+        g.profile_tiled_kernel(True)
+        clocks = ClockSampler(local_rank)
+        clocks.start()
+        launches0 = g.kernel_launches()
+        ms = timed(step_device, args.steps)
+        launches = g.kernel_launches() - launches0
+        csum = clocks.stop()
+        g.profile_tiled_kernel(False)
+        kms, kcount = g.tiled_kernel_time()
+        ms_step = ms / args.steps
+        k_avg = kms / kcount if kcount else None
+        results[form] = {
+            "value": total_vis / (ms_step * 1e-3) / 1e6,
+            "ms_per_step": ms_step,
+            "kernel_ms": k_avg, "kernel_launches": kcount,
+            "gpu_launches": launches,
+            "step_gbs": b_alg / (ms_step * 1e-3) / 1e9,
+            "kernel_gbs": (b_kernel / (k_avg * 1e-3) / 1e9) if k_avg else None,
+            "clocks": csum,
+        }
+        if form == forms[0]:
+            clock_summary = csum
+
+    head = results[forms[0]]
+    e2e_value = None
     if not args.no_e2e:
+        g.set_precision(hpg_b200.PRECISION_MIXED if forms[0] == "mixed"
+                        else hpg_b200.PRECISION_FP64)
+        e2e_steps = max(1, min(args.steps, 3))
         step_e2e()
         ms_e2e = timed(step_e2e, e2e_steps)
+        e2e_value = total_vis / (ms_e2e / e2e_steps * 1e-3) / 1e6
 
-    ms_step = ms / args.steps
-    total_vis = args.nvis * world
-    value = total_vis / (ms_step * 1e-3) / 1e6
-    e2e_value = (total_vis / (ms_e2e / e2e_steps * 1e-3) / 1e6
-                 if ms_e2e else None)
-
-    taps = taps_of(p["supports"])
-    b_alg = workloads.algorithmic_bytes(vis, 4, taps, 16,
-                                        int(np.prod(wl["grid_size"])), 3)
-    peak, peak_kind = peaks()
-    achieved = b_alg / (ms_step * 1e-3) / 1e9
+    # full-size error of the mixed form against the FP64 form (one step each
+    # from a zero grid; the FP64 form is checked against the CPU oracle by
+    # the parity tests)
+    mixed_err = None
+    if "mixed" in results and "fp64" in results:
+        grids = {}
+        for form in ("fp64", "mixed"):
+            g.set_precision(hpg_b200.PRECISION_MIXED if form == "mixed"
+                            else hpg_b200.PRECISION_FP64)
+            g.reset_grid()
+            step_device()
+            g.fence()
+            grids[form] = (g.grid_values(), g.grid_weights())
+        gf, wf = grids["fp64"]
+        gm, wm = grids["mixed"]
+        mixed_err = {
+            "grid_rel": float(np.linalg.norm((gm - gf).ravel()) /
+                              np.linalg.norm(gf.ravel())),
+            "weights_rel": float(np.linalg.norm(wm - wf) / np.linalg.norm(wf)),
+        }
+        del grids, gf, gm
 
     cpu = None
     if cpu_wl is not None:
@@ -341,29 +405,46 @@ def main():
                    "sample": f"failed: {e}"}
 
     if rank == 0:
+        kernel_gbs = head["kernel_gbs"]
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "metric": METRIC, "value": head["value"], "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": head["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32-mixed",
+            "dtype": "f64" if forms[0] == "fp64" else "f32-mixed",
             "data": "synthetic",
             "config": {
                 "workload": "full-pol degrid+grid 2048x2048x4, 8 CF groups "
                             "(supports 8-32, os 128), dense 4x4 Mueller",
                 "nvis": args.nvis, "grid": list(wl["grid_size"]),
-                "precision": args.precision,
+                "precision": forms[0],
                 "l2": "inputs larger than L2 (CF 10 GB, visibilities 1.2 GB)",
                 "parallelism": f"replicas x{world}"},
+            "forms": results,
+            "mixed_over_fp64": (results["mixed"]["value"] /
+                                results["fp64"]["value"]
+                                if len(results) == 2 else None),
+            "mixed_vs_fp64_error": mixed_err,
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": int(vis.nbytes),
                     "d2h_bytes_per_step": int(np.prod(wl["grid_size"][2:]) * 8)},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": None,
+            "roofline": {"bound": "hbm", "kernel": "tiled_kernel",
+                         "achieved": kernel_gbs, "peak": peak,
+                         "unit": "GB/s",
+                         "frac": kernel_gbs / peak if kernel_gbs else None,
+                         "peak_kind": peak_kind,
+                         "traffic": kernel_traffic(forms[0], args.nvis,
+                                                   grid_elems),
+                         "traffic_source": "ncu capture, 200k visibilities "
+                                           "at CF oversampling 64, scaled by "
+                                           "visibility count",
+                         "algorithmic_bytes_per_launch": b_kernel,
+                         "step_achieved": head["step_gbs"],
+                         "step_frac": head["step_gbs"] / peak,
                          "algorithmic_bytes_per_step": b_alg},
             "cpu_baseline": cpu,
             "clocks": clock_summary,
-            "gpu_launches": launches,
+            "gpu_launches": head["gpu_launches"],
         }
         print(json.dumps(line), flush=True)
     g.close()

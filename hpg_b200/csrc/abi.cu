@@ -269,6 +269,10 @@ int hpgb_destroy(hpgb_gridder* g) {
     cudaSetDevice(g->device);
     cudaStreamSynchronize(g->stream);
     release_fft_plans(g);
+    for (auto& e : g->prof_events) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
     cudaStream_t s = g->stream;
     delete g;  // DevBuf destructors free device memory
     if (s) cudaStreamDestroy(s);
@@ -616,6 +620,41 @@ int hpgb_kernel_launches(const hpgb_gridder* g, uint64_t* count) {
     if (!g || !count) return Status::err(HPGB_ERROR_OTHER, "null argument");
     *count = g->launches;
     return Status::ok();
+  });
+}
+
+int hpgb_profile_tiled_kernel(hpgb_gridder* g, int enable) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    g->profile = enable != 0;
+    return Status::ok();
+  });
+}
+
+int hpgb_tiled_kernel_time(hpgb_gridder* g, double* total_ms,
+                           uint64_t* count) {
+  return guarded([&]() -> Status {
+    if (!g || !total_ms || !count)
+      return Status::err(HPGB_ERROR_OTHER, "null argument");
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    double sum = 0.0;
+    Status st = Status::ok();
+    for (auto& e : g->prof_events) {
+      float ms = 0.f;
+      const cudaError_t rc = cudaEventElapsedTime(&ms, e.first, e.second);
+      if (rc != cudaSuccess && st)
+        st = Status::err(HPGB_ERROR_OTHER,
+                         std::string("cudaEventElapsedTime: ") +
+                             cudaGetErrorString(rc));
+      sum += ms;
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    *count = g->prof_events.size();
+    *total_ms = sum;
+    g->prof_events.clear();
+    return st;
   });
 }
 

@@ -1150,8 +1150,18 @@ Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
     cfg.gridDim = dim3(unsigned(max_clusters * p.nrow));
   else
     cudaGetLastError();
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  if (g->profile) {
+    HPGB_CUDA_TRY(cudaEventCreate(&ev[0]));
+    HPGB_CUDA_TRY(cudaEventCreate(&ev[1]));
+    HPGB_CUDA_TRY(cudaEventRecord(ev[0], g->stream));
+  }
   HPGB_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, p, map));
   ++g->launches;
+  if (g->profile) {
+    HPGB_CUDA_TRY(cudaEventRecord(ev[1], g->stream));
+    g->prof_events.emplace_back(ev[0], ev[1]);
+  }
   return Status::ok();
 }
 

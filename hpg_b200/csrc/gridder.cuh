@@ -7,6 +7,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -84,6 +85,11 @@ struct hpgb_gridder {
 
   mutable std::mutex mtx;
   uint64_t launches = 0;  // kernels launched by this gridder
+
+  // event pairs around each launch of the tiled gridding kernel, recorded
+  // while profiling is on (benchmark instrumentation)
+  bool profile = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
 
   size_t grid_elems() const {
     return size_t(grid_size[0]) * grid_size[1] * grid_size[2] * grid_size[3];

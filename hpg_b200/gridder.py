@@ -332,6 +332,20 @@ class Gridder:
     def shift_model(self, direction=abi.SHIFT_FORWARD):
         check(load().hpgb_shift_model(self._h, int(direction)))
 
+    def profile_tiled_kernel(self, enable=True):
+        """Record CUDA events around every tiled-kernel launch (benchmark
+        instrumentation)."""
+        check(load().hpgb_profile_tiled_kernel(self._h, int(bool(enable))))
+
+    def tiled_kernel_time(self):
+        """(summed device ms, launches) of the tiled-kernel launches recorded
+        since the last call; waits for the gridder's stream."""
+        ms = ctypes.c_double()
+        n = ctypes.c_uint64()
+        check(load().hpgb_tiled_kernel_time(self._h, ctypes.byref(ms),
+                                            ctypes.byref(n)))
+        return ms.value, n.value
+
     def kernel_launches(self):
         """Kernels this gridder has launched so far."""
         n = ctypes.c_uint64()

@@ -297,6 +297,15 @@ HPGB_API int hpgb_shift_model(hpgb_gridder* gridder, int direction);
 HPGB_API int hpgb_kernel_launches(const hpgb_gridder* gridder,
                                   uint64_t* count);
 
+/* Benchmark instrumentation, no counterpart in the reference: while
+ * enabled, CUDA events are recorded on the gridder's stream around every
+ * launch of the tiled gridding kernel.  hpgb_tiled_kernel_time waits for the
+ * stream, returns the summed device time (ms) and the number of launches
+ * recorded since the last query, and forgets them. */
+HPGB_API int hpgb_profile_tiled_kernel(hpgb_gridder* gridder, int enable);
+HPGB_API int hpgb_tiled_kernel_time(hpgb_gridder* gridder, double* total_ms,
+                                    uint64_t* count);
+
 /* Debug: coordinates the device computes for each visibility (host input,
  * host output), for bit-exact comparison with the reference's
  * compute_vis_coord().  No counterpart in the reference's State. */
