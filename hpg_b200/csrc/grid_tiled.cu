@@ -96,7 +96,8 @@ struct alignas(16) TileDesc {
   double2 wfac[4];       // conj(phasor) / normaliser, per polarization
   double twgt[4];        // grid weight increment per grid row
   float2 gvis[4];        // values scaled for gridding (used without degrid)
-  int32_t pad1[4];
+  float inv_tx;          // 1 / taps_x, rounded to float
+  int32_t pad1[3];
 };
 static_assert(sizeof(TileDesc) == 256, "TileDesc is one 256-byte bulk copy");
 
@@ -307,7 +308,8 @@ __global__ void tile_desc_kernel(const VisData<N>* vis, const unsigned* order,
       }
     d.twgt[r] = tw;
   }
-  for (int k = 0; k < 4; ++k) d.pad1[k] = 0;
+  d.inv_tx = 1.0f / float(vc.taps[0]);
+  for (int k = 0; k < 3; ++k) d.pad1[k] = 0;
   descs[pidx] = d;
   SliceRef s;
   s.off = (G.data - cf_base) + sidx * G.slice_stride;
@@ -347,6 +349,7 @@ struct Form<true> {
 // into registers once per visibility.
 struct VisGeom {
   int cx, cy, tx, ty, pst;
+  float inv_tx;
   bool pos_w, screen_on;
   double phi0x, phi0y, dphix, dphiy;
 };
@@ -358,124 +361,153 @@ __device__ __forceinline__ VisGeom vis_geom(const TileDesc& d) {
   v.tx = d.taps_x;
   v.ty = d.taps_y;
   v.pst = d.pstride;
+  v.inv_tx = d.inv_tx;
   v.pos_w = d.flags & kPosW;
   v.screen_on = d.flags & kScreen;
-  v.phi0x = d.phi0[0];
-  v.phi0y = d.phi0[1];
-  v.dphix = d.dphi[0];
-  v.dphiy = d.dphi[1];
+  v.phi0x = v.phi0y = v.dphix = v.dphiy = 0.0;
+  if (v.screen_on) {
+    v.phi0x = d.phi0[0];
+    v.phi0y = d.phi0[1];
+    v.dphix = d.dphi[0];
+    v.dphiy = d.dphi[1];
+  }
   return v;
 }
 
+// Footprint cells c = first, first + stride, ... with their (X, Y), advanced
+// without integer division: the start and the step are split with the
+// float reciprocal of taps_x, exact here because c + 0.5 < 2^12 and
+// taps_x < 128 keep the rounding error (< 5e-4) below the distance of
+// (c + 0.5) / taps_x to the nearest integer (>= 0.5 / taps_x).
+struct CellWalk {
+  int X, Y, dX, dY;
+  __device__ __forceinline__ CellWalk(int first, int stride, int tx,
+                                      float inv_tx) {
+    Y = int((float(first) + 0.5f) * inv_tx);
+    X = first - Y * tx;
+    dY = int((float(stride) + 0.5f) * inv_tx);
+    dX = stride - dY * tx;
+  }
+  __device__ __forceinline__ void next(int tx) {
+    X += dX;
+    Y += dY;
+    if (X >= tx) {
+      X -= tx;
+      ++Y;
+    }
+  }
+};
+
 // Partial degridding sums of this CTA's row over the footprint cells
 // c = first, first + stride, ... of one visibility (src/hpg_core.hpp:642-668).
-// pp[v]: slot plane of Mueller element dmi[row][v] (-1 if inactive).
-template <int N, bool MIXED>
+// pp[v]: slot plane of Mueller element dmi[row][v] (-1 if inactive; never
+// when DENSE).  The sign of the CF imaginary part (+1 for w > 0, else -1)
+// is moved onto the model value's imaginary part and the sum's imaginary
+// part: sgn*(cf * m) with cf' = (cr, sgn*ci) equals the sum taken with
+// (cr, ci) and (mx, sgn*my), imaginary part times sgn, bit for bit.
+template <int N, bool MIXED, bool DENSE>
 __device__ __forceinline__ void degrid_cells(
     const VisGeom& g, const int (&pp)[N], const float2* __restrict__ cfs,
     const typename Form<MIXED>::model_t* __restrict__ mtile, int R, int first,
     int stride, double (&acc)[2 * N]) {
-  const int tx = g.tx, ncell = g.tx * g.ty, pst = g.pst;
-  const float im = g.pos_w ? 1.0f : -1.0f;
-  // (X, Y) of cell `first`, advanced incrementally
-  int Y = first / tx, X = first - Y * tx;
-  const int dY = stride / tx, dX = stride - dY * tx;
+  const int tx = g.tx, ncell = g.tx * g.ty;
+  CellWalk w(first, stride, tx, g.inv_tx);
+  const float2* cfv[N];
+#pragma unroll
+  for (int v = 0; v < N; ++v) cfv[v] = cfs + (pp[v] >= 0 ? pp[v] : 0) * g.pst;
   const typename Form<MIXED>::model_t* mrow = mtile + g.cy * R + g.cx;
   if constexpr (!MIXED) {
+    const double sgn = g.pos_w ? 1.0 : -1.0;
     for (int c = first; c < ncell; c += stride) {
-      double2 mv = mrow[Y * R + X];
+      double2 mv = mrow[w.Y * R + w.X];
       if (g.screen_on) {
-        const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(X), g.dphix));
-        const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(Y), g.dphiy));
+        const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(w.X), g.dphix));
+        const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(w.Y), g.dphiy));
         mv = cmul_d(mv, cphase_d(__dsub_rn(-phx, phy)));
       }
+      const double my = sgn * mv.y;
 #pragma unroll
       for (int v = 0; v < N; ++v) {
-        if (pp[v] >= 0) {
-          const float2 cf = cfs[pp[v] * pst + c];
-          const double cr = cf.x, ci = double(cf.y * im);
-          acc[2 * v] = fma(cr, mv.x, fma(-ci, mv.y, acc[2 * v]));
-          acc[2 * v + 1] = fma(cr, mv.y, fma(ci, mv.x, acc[2 * v + 1]));
+        if (DENSE || pp[v] >= 0) {
+          const float2 cf = cfv[v][c];
+          const double cr = cf.x, ci = cf.y;
+          acc[2 * v] = fma(cr, mv.x, fma(-ci, my, acc[2 * v]));
+          acc[2 * v + 1] = fma(cr, my, fma(ci, mv.x, acc[2 * v + 1]));
         }
       }
-      X += dX;
-      Y += dY;
-      if (X >= tx) {
-        X -= tx;
-        ++Y;
-      }
+      w.next(tx);
     }
+#pragma unroll
+    for (int v = 0; v < N; ++v) acc[2 * v + 1] *= sgn;
   } else {
+    const float sgn = g.pos_w ? 1.0f : -1.0f;
     float a[2 * N];
 #pragma unroll
     for (int k = 0; k < 2 * N; ++k) a[k] = 0.f;
     for (int c = first; c < ncell; c += stride) {
-      float2 mv = mrow[Y * R + X];
+      float2 mv = mrow[w.Y * R + w.X];
       if (g.screen_on) {
-        const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(X), g.dphix));
-        const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(Y), g.dphiy));
+        const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(w.X), g.dphix));
+        const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(w.Y), g.dphiy));
         const double2 sc = cphase_d(__dsub_rn(-phx, phy));
         const float sx = float(sc.x), sy = float(sc.y);
         mv = make_float2(mv.x * sx - mv.y * sy, mv.x * sy + mv.y * sx);
       }
+      const float my = sgn * mv.y;
 #pragma unroll
       for (int v = 0; v < N; ++v) {
-        if (pp[v] >= 0) {
-          const float2 cf = cfs[pp[v] * pst + c];
-          const float ci = cf.y * im;
-          a[2 * v] = fmaf(cf.x, mv.x, fmaf(-ci, mv.y, a[2 * v]));
-          a[2 * v + 1] = fmaf(cf.x, mv.y, fmaf(ci, mv.x, a[2 * v + 1]));
+        if (DENSE || pp[v] >= 0) {
+          const float2 cf = cfv[v][c];
+          a[2 * v] = fmaf(cf.x, mv.x, fmaf(-cf.y, my, a[2 * v]));
+          a[2 * v + 1] = fmaf(cf.x, my, fmaf(cf.y, mv.x, a[2 * v + 1]));
         }
       }
-      X += dX;
-      Y += dY;
-      if (X >= tx) {
-        X -= tx;
-        ++Y;
-      }
+      w.next(tx);
     }
 #pragma unroll
-    for (int k = 0; k < 2 * N; ++k) acc[k] = a[k];
+    for (int v = 0; v < N; ++v) {
+      acc[2 * v] = a[2 * v];
+      acc[2 * v + 1] = double(a[2 * v + 1]) * double(sgn);
+    }
   }
 }
 
-// Gridding of one visibility into the rows of the grid tile owned by warp
-// `gw` (tile rows congruent to gw modulo kGR), so that different warps never
-// write the same tile cell (src/hpg_core.hpp:856-873).
-// pp[v]: slot plane of Mueller element gmi[row][v] (-1 if inactive).
-template <int N, bool MIXED>
-__device__ __forceinline__ void grid_rows(
+// Gridding of one visibility's footprint cells c = first, first + stride,
+// ... into the row's shared-memory grid tile (src/hpg_core.hpp:856-873).
+// The gridding warps cover every cell of one visibility between two
+// barriers, so no two threads add to a tile cell at once.  pp[v]: slot
+// plane of Mueller element gmi[row][v] (-1 if inactive; never when DENSE).
+// gv[v] arrive conjugated when w > 0 (the CF imaginary part is negated
+// then): conj(cf)*s*g = conj(cf*conj(s)*conj(g)), bit for bit in the
+// reference's FP32 products, so only the sum's imaginary part flips.
+template <int N, bool MIXED, bool DENSE>
+__device__ __forceinline__ void grid_cells(
     const VisGeom& g, const int (&pp)[N], const float2* __restrict__ cfs,
     const float2 (&gv)[N], typename Form<MIXED>::grid_t* __restrict__ gtile,
-    int R, int gw, int lane) {
-  const int tx = g.tx, ty = g.ty, pst = g.pst;
-  const float im = g.pos_w ? -1.0f : 1.0f;
-  const int Y0 = (gw - g.cy % kGR + kGR) % kGR;  // first footprint row owned
-  if (Y0 >= ty) return;
-  const int nr = (ty - Y0 + kGR - 1) / kGR;
-  const int ncw = nr * tx;  // cells of this warp
-  // flattened index i -> (row r_i, X); footprint row Y = Y0 + r_i*kGR
-  int ri = lane / tx, X = lane - ri * tx;
-  const int dR = 32 / tx, dX = 32 - dR * tx;
+    int R, int first, int stride) {
+  const int tx = g.tx, ncell = g.tx * g.ty;
+  CellWalk w(first, stride, tx, g.inv_tx);
+  const float2* cfv[N];
+#pragma unroll
+  for (int v = 0; v < N; ++v) cfv[v] = cfs + (pp[v] >= 0 ? pp[v] : 0) * g.pst;
   typename Form<MIXED>::grid_t* gbase = gtile + g.cy * R + g.cx;
-  for (int i = lane; i < ncw; i += 32) {
-    const int Y = Y0 + ri * kGR;
-    const int c = Y * tx + X;
+  for (int c = first; c < ncell; c += stride) {
     float2 screen = make_float2(1.0f, 0.0f);
     if (g.screen_on) {
-      const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(X), g.dphix));
-      const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(Y), g.dphiy));
+      const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(w.X), g.dphix));
+      const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(w.Y), g.dphiy));
       const double2 sc = cphase_d(__dadd_rn(phx, phy));
-      screen = make_float2(__double2float_rn(sc.x), __double2float_rn(sc.y));
+      screen = make_float2(__double2float_rn(sc.x),
+                           g.pos_w ? -__double2float_rn(sc.y)
+                                   : __double2float_rn(sc.y));
     }
-    const int idx = Y * R + X;
+    const int idx = w.Y * R + w.X;
     if constexpr (!MIXED) {
       double sx = 0.0, sy = 0.0;
 #pragma unroll
       for (int v = 0; v < N; ++v) {
-        if (pp[v] >= 0) {
-          float2 cf = cfs[pp[v] * pst + c];
-          cf.y *= im;
+        if (DENSE || pp[v] >= 0) {
+          const float2 cf = cfv[v][c];
           const float2 prod = g.screen_on ? cmul_f(cmul_f(cf, screen), gv[v])
                                           : cmul_f(cf, gv[v]);
           sx = __dadd_rn(sx, double(prod.x));
@@ -484,15 +516,14 @@ __device__ __forceinline__ void grid_rows(
       }
       double2 t = gbase[idx];
       t.x += sx;
-      t.y += sy;
+      t.y = g.pos_w ? t.y - sy : t.y + sy;
       gbase[idx] = t;
     } else {
       float sx = 0.f, sy = 0.f;
 #pragma unroll
       for (int v = 0; v < N; ++v) {
-        if (pp[v] >= 0) {
-          float2 cf = cfs[pp[v] * pst + c];
-          cf.y *= im;
+        if (DENSE || pp[v] >= 0) {
+          float2 cf = cfv[v][c];
           if (g.screen_on)
             cf = make_float2(cf.x * screen.x - cf.y * screen.y,
                              cf.x * screen.y + cf.y * screen.x);
@@ -502,19 +533,14 @@ __device__ __forceinline__ void grid_rows(
       }
       float2 t = gbase[idx];
       t.x += sx;
-      t.y += sy;
+      t.y = g.pos_w ? t.y - sy : t.y + sy;
       gbase[idx] = t;
     }
-    X += dX;
-    ri += dR;
-    if (X >= tx) {
-      X -= tx;
-      ++ri;
-    }
+    w.next(tx);
   }
 }
 
-template <int N, bool MIXED>
+template <int N, bool MIXED, bool DENSE>
 __global__ void __launch_bounds__(kThreadsTiled, 1)
 tiled_kernel(const __grid_constant__ TiledParams p,
              const __grid_constant__ CUtensorMap model_map) {
@@ -747,7 +773,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
 #pragma unroll
             for (int v = 0; v < N; ++v)
               pp[v] = int(int8_t((vg.pos_w ? dpk[1] : dpk[0]) >> (8 * v)));
-            degrid_cells<N, MIXED>(
+            degrid_cells<N, MIXED, DENSE>(
                 vg, pp, reinterpret_cast<const float2*>(ring + ring_off[s]),
                 mtile, R, warp * 32 + lane, kDG * 32, acc);
           }
@@ -902,6 +928,9 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         }
       } else {
         // -------- gridding warps --------
+        // All gridding warps cover the cells of one visibility between two
+        // barriers (id 2), so footprints of consecutive visibilities that
+        // overlap are never added to the tile at the same time.
         const int gw = warp - kGRBase;
         for (int k = 0; k < ch.count; ++k, ++q) {
           const int s = int(q % uint32_t(kSlots));
@@ -912,6 +941,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             const int gs = int(q % uint32_t(kSlots));
             TT_BEGIN();
             ok &= ptx::mbar_wait(&gvfull[gs], (q / kSlots) & 1, abort);
+            if (k > 0) ptx::named_sync(2, kGR * 32);
             TT_END(6);
             TT_BEGIN();
             if (!ptx::warp_flag(abort)) {
@@ -922,10 +952,11 @@ tiled_kernel(const __grid_constant__ TiledParams p,
               for (int v = 0; v < N; ++v) {
                 pp[v] = int(int8_t((vg.pos_w ? gpk[1] : gpk[0]) >> (8 * v)));
                 gv[v] = gvring[gs * 4 + v];
+                if (vg.pos_w) gv[v].y = -gv[v].y;
               }
-              grid_rows<N, MIXED>(
+              grid_cells<N, MIXED, DENSE>(
                   vg, pp, reinterpret_cast<const float2*>(ring + ring_off[s]),
-                  gv, gtile, R, gw, lane);
+                  gv, gtile, R, gw * 32 + lane, kGR * 32);
             }
             TT_END(7);
           }
@@ -1126,7 +1157,14 @@ Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
   if ((p.do_degrid && p.has_model && p.esize_model == 0) ||
       (p.do_grid && p.esize_grid == 0))
     return Status::err(HPGB_ERROR_OTHER, "tiled kernel tile missing");
-  auto kern = tiled_kernel<N, MIXED>;
+  // every Mueller element of every row active: the cell loops skip the
+  // per-element activity test
+  bool dense = true;
+  for (int r = 0; r < p.nrow; ++r)
+    for (int w = 0; w < 2; ++w)
+      for (int v = 0; v < N; ++v)
+        dense = dense && p.dpos[r][w][v] >= 0 && p.gpos[r][w][v] >= 0;
+  auto kern = dense ? tiled_kernel<N, MIXED, true> : tiled_kernel<N, MIXED, false>;
   HPGB_CUDA_TRY(cudaFuncSetAttribute(
       kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   cudaLaunchConfig_t cfg = {};
