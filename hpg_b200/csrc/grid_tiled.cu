@@ -16,23 +16,27 @@
 //                         weights from the per-slice CF sums, gridding
 //                         values) + the address of its CF slice
 //   5. tiled_kernel       persistent, one thread-block cluster per tile with
-//                         one CTA per grid row (Mueller row) r:
+//                         one CTA per grid row (Mueller row) r; 19 warps:
 //                         - a producer warp streams each visibility's
 //                           descriptor and the CF planes row r needs
 //                           (Mueller row r of both index sets) into a ring of
-//                           shared-memory slots with cp.async.bulk, mbarrier
-//                           completion, and prefetches later slices into L2;
+//                           shared-memory slots with cp.async.bulk and
+//                           mbarrier completion (16 visibilities in flight
+//                           at most, bounded by the ring's bytes);
 //                         - the model tile of row r is loaded once per chunk
 //                           with a 3-D TMA tensor copy;
-//                         - 8 consumer warps degrid the visibility against
-//                           the model tile (partial sums of row r), exchange
-//                           the partials with the other rows' CTAs through
+//                         - 8 degridding warps in two groups of 4 take
+//                           alternate visibilities: partial sums of row r
+//                           over the footprint, reduced per warp;
+//                         - 2 exchange warps (alternate visibilities) send
+//                           the partials to every CTA of the cluster through
 //                           distributed shared memory and a remote mbarrier,
-//                           form the prediction and residual (identically in
-//                           every CTA), and grid the scaled residual into the
-//                           row's shared-memory grid tile; visibility j is
-//                           finished and gridded while the partials of j+1
-//                           travel (four exchange buffers in flight);
+//                           and form the prediction, residual and gridding
+//                           values (identically in every CTA), finishing
+//                           visibility q after sending those of q + 2;
+//                         - 8 gridding warps add the scaled residual of one
+//                           visibility at a time into the row's
+//                           shared-memory grid tile;
 //                         - at the end of a chunk the tile is added to the
 //                           FP64 grid with red.global.add.f64, and the row's
 //                           weight sum to the weights.
@@ -71,6 +75,12 @@ namespace {
 // warp roles of the tiled kernel: kDG degridding warps, kX exchange warps
 // (alternating visibilities), kGR gridding warps, one producer warp
 constexpr int kDG = 8;
+// the degridding warps form two groups of four that take alternate
+// visibilities, as the two exchange warps do: two visibilities are degridded
+// at once, so a group's per-visibility latency (loads, warp reduction,
+// hand-off) overlaps the other group's work
+constexpr int kDGGroups = 2;
+constexpr int kDGPer = kDG / kDGGroups;
 constexpr int kX = 2;
 constexpr int kGR = 8;
 constexpr int kXBase = kDG;
@@ -78,8 +88,9 @@ constexpr int kGRBase = kXBase + kX;
 constexpr int kPWarp = kGRBase + kGR;
 constexpr int kXSlots = 8;  // exchange buffers (visibility q uses q % 8)
 constexpr int kConsumers = (kDG + kX + kGR) * 32;
+static_assert(kDGGroups == kX, "degridding group g hands visibilities to exchange warp g");
 constexpr int kThreadsTiled = kConsumers + 32;
-constexpr int kSlots = 8;  // descriptor slots (visibilities in flight)
+constexpr int kSlots = 16;  // descriptor slots (visibilities in flight)
 constexpr int kChunkVisFP64 = 2048;
 constexpr int kChunkVisMixed = 256;
 constexpr int kMaxRuns = 8;
@@ -168,10 +179,10 @@ __host__ __device__ inline SmemLayout smem_layout(int ring_bytes, int R,
                                                   int esize_model,
                                                   int esize_grid) {
   SmemLayout L;
-  // 37 mbarriers: full[8] empty[8] model xchg[8] dgfull[2] dgempty[2]
-  // gvfull[8], then the abort flag
+  // mbarriers full[kSlots] empty[kSlots] model xchg[kXSlots] dgfull[2]
+  // dgempty[2] gvfull[kSlots], then the abort flag
   L.bars = 0;
-  L.xbuf = 320;                       // [8][4 rows][4 pol] complex double
+  L.xbuf = align_up((3 * kSlots + kXSlots + 5) * 8 + 8, 16);  // [kXSlots][4 rows][4 pol] complex double
   L.wred = L.xbuf + kXSlots * 4 * 4 * 16;  // [2][kDG][8] double (degrid partials)
   L.bcast = L.wred + 2 * kDG * 8 * 8; // [kSlots][4] float2 (gridding values)
   L.slots = L.bcast + kSlots * 4 * 8;  // ring_off[kSlots] int, slot_end[kSlots] u64
@@ -374,26 +385,34 @@ __device__ __forceinline__ VisGeom vis_geom(const TileDesc& d) {
   return v;
 }
 
-// Footprint cells c = first, first + stride, ... with their (X, Y), advanced
-// without integer division: the start and the step are split with the
-// float reciprocal of taps_x, exact here because c + 0.5 < 2^12 and
-// taps_x < 128 keep the rounding error (< 5e-4) below the distance of
-// (c + 0.5) / taps_x to the nearest integer (>= 0.5 / taps_x).
+// Footprint cells c = first, first + stride, ... with their (X, Y) and the
+// shared-memory address of their tile cell (row pitch R elements of `esize`
+// bytes), advanced without integer division: the start and the step are
+// split with the float reciprocal of taps_x, exact here because
+// c + 0.5 < 2^12 and taps_x < 128 keep the rounding error (< 5e-4) below the
+// distance of (c + 0.5) / taps_x to the nearest integer (>= 0.5 / taps_x).
 struct CellWalk {
   int X, Y, dX, dY;
+  uint32_t tile, dtile, wrap;  // tile-cell address, its step, row wrap
   __device__ __forceinline__ CellWalk(int first, int stride, int tx,
-                                      float inv_tx) {
+                                      float inv_tx, uint32_t tile0, int R,
+                                      uint32_t esize) {
     Y = int((float(first) + 0.5f) * inv_tx);
     X = first - Y * tx;
     dY = int((float(stride) + 0.5f) * inv_tx);
     dX = stride - dY * tx;
+    tile = tile0 + uint32_t(Y * R + X) * esize;
+    dtile = uint32_t(dY * R + dX) * esize;
+    wrap = uint32_t(R - tx) * esize;
   }
   __device__ __forceinline__ void next(int tx) {
     X += dX;
     Y += dY;
+    tile += dtile;
     if (X >= tx) {
       X -= tx;
       ++Y;
+      tile += wrap;
     }
   }
 };
@@ -405,22 +424,25 @@ struct CellWalk {
 // is moved onto the model value's imaginary part and the sum's imaginary
 // part: sgn*(cf * m) with cf' = (cr, sgn*ci) equals the sum taken with
 // (cr, ci) and (mx, sgn*my), imaginary part times sgn, bit for bit.
-template <int N, bool MIXED, bool DENSE>
+template <int N, bool MIXED, bool DENSE, bool SCREEN>
 __device__ __forceinline__ void degrid_cells(
-    const VisGeom& g, const int (&pp)[N], const float2* __restrict__ cfs,
-    const typename Form<MIXED>::model_t* __restrict__ mtile, int R, int first,
-    int stride, double (&acc)[2 * N]) {
+    const VisGeom& g, const int (&pp)[N], uint32_t cfs, uint32_t mtile, int R,
+    int first, int stride, double (&acc)[2 * N]) {
+  using MT = typename Form<MIXED>::model_t;
   const int tx = g.tx, ncell = g.tx * g.ty;
-  CellWalk w(first, stride, tx, g.inv_tx);
-  const float2* cfv[N];
+  CellWalk w(first, stride, tx, g.inv_tx,
+             mtile + uint32_t(g.cy * R + g.cx) * uint32_t(sizeof(MT)), R,
+             uint32_t(sizeof(MT)));
+  uint32_t po[N];  // plane offsets in bytes
 #pragma unroll
-  for (int v = 0; v < N; ++v) cfv[v] = cfs + (pp[v] >= 0 ? pp[v] : 0) * g.pst;
-  const typename Form<MIXED>::model_t* mrow = mtile + g.cy * R + g.cx;
+  for (int v = 0; v < N; ++v) po[v] = uint32_t((pp[v] >= 0 ? pp[v] : 0) * g.pst) * 8u;
+  uint32_t ca = cfs + uint32_t(first) * 8u;
+  const uint32_t dca = uint32_t(stride) * 8u;
   if constexpr (!MIXED) {
     const double sgn = g.pos_w ? 1.0 : -1.0;
     for (int c = first; c < ncell; c += stride) {
-      double2 mv = mrow[w.Y * R + w.X];
-      if (g.screen_on) {
+      double2 mv = ptx::lds_d2(w.tile);
+      if constexpr (SCREEN) {
         const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(w.X), g.dphix));
         const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(w.Y), g.dphiy));
         mv = cmul_d(mv, cphase_d(__dsub_rn(-phx, phy)));
@@ -429,13 +451,14 @@ __device__ __forceinline__ void degrid_cells(
 #pragma unroll
       for (int v = 0; v < N; ++v) {
         if (DENSE || pp[v] >= 0) {
-          const float2 cf = cfv[v][c];
+          const float2 cf = ptx::lds_f2(ca + po[v]);
           const double cr = cf.x, ci = cf.y;
           acc[2 * v] = fma(cr, mv.x, fma(-ci, my, acc[2 * v]));
           acc[2 * v + 1] = fma(cr, my, fma(ci, mv.x, acc[2 * v + 1]));
         }
       }
       w.next(tx);
+      ca += dca;
     }
 #pragma unroll
     for (int v = 0; v < N; ++v) acc[2 * v + 1] *= sgn;
@@ -445,8 +468,8 @@ __device__ __forceinline__ void degrid_cells(
 #pragma unroll
     for (int k = 0; k < 2 * N; ++k) a[k] = 0.f;
     for (int c = first; c < ncell; c += stride) {
-      float2 mv = mrow[w.Y * R + w.X];
-      if (g.screen_on) {
+      float2 mv = ptx::lds_f2(w.tile);
+      if constexpr (SCREEN) {
         const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(w.X), g.dphix));
         const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(w.Y), g.dphiy));
         const double2 sc = cphase_d(__dsub_rn(-phx, phy));
@@ -457,12 +480,13 @@ __device__ __forceinline__ void degrid_cells(
 #pragma unroll
       for (int v = 0; v < N; ++v) {
         if (DENSE || pp[v] >= 0) {
-          const float2 cf = cfv[v][c];
+          const float2 cf = ptx::lds_f2(ca + po[v]);
           a[2 * v] = fmaf(cf.x, mv.x, fmaf(-cf.y, my, a[2 * v]));
           a[2 * v + 1] = fmaf(cf.x, my, fmaf(cf.y, mv.x, a[2 * v + 1]));
         }
       }
       w.next(tx);
+      ca += dca;
     }
 #pragma unroll
     for (int v = 0; v < N; ++v) {
@@ -480,20 +504,24 @@ __device__ __forceinline__ void degrid_cells(
 // gv[v] arrive conjugated when w > 0 (the CF imaginary part is negated
 // then): conj(cf)*s*g = conj(cf*conj(s)*conj(g)), bit for bit in the
 // reference's FP32 products, so only the sum's imaginary part flips.
-template <int N, bool MIXED, bool DENSE>
-__device__ __forceinline__ void grid_cells(
-    const VisGeom& g, const int (&pp)[N], const float2* __restrict__ cfs,
-    const float2 (&gv)[N], typename Form<MIXED>::grid_t* __restrict__ gtile,
-    int R, int first, int stride) {
+template <int N, bool MIXED, bool DENSE, bool SCREEN>
+__device__ __forceinline__ void grid_cells(const VisGeom& g, const int (&pp)[N],
+                                           uint32_t cfs, const float2 (&gv)[N],
+                                           uint32_t gtile, int R, int first,
+                                           int stride) {
+  using GT = typename Form<MIXED>::grid_t;
   const int tx = g.tx, ncell = g.tx * g.ty;
-  CellWalk w(first, stride, tx, g.inv_tx);
-  const float2* cfv[N];
+  CellWalk w(first, stride, tx, g.inv_tx,
+             gtile + uint32_t(g.cy * R + g.cx) * uint32_t(sizeof(GT)), R,
+             uint32_t(sizeof(GT)));
+  uint32_t po[N];
 #pragma unroll
-  for (int v = 0; v < N; ++v) cfv[v] = cfs + (pp[v] >= 0 ? pp[v] : 0) * g.pst;
-  typename Form<MIXED>::grid_t* gbase = gtile + g.cy * R + g.cx;
+  for (int v = 0; v < N; ++v) po[v] = uint32_t((pp[v] >= 0 ? pp[v] : 0) * g.pst) * 8u;
+  uint32_t ca = cfs + uint32_t(first) * 8u;
+  const uint32_t dca = uint32_t(stride) * 8u;
   for (int c = first; c < ncell; c += stride) {
     float2 screen = make_float2(1.0f, 0.0f);
-    if (g.screen_on) {
+    if constexpr (SCREEN) {
       const double phx = __dadd_rn(g.phi0x, __dmul_rn(double(w.X), g.dphix));
       const double phy = __dadd_rn(g.phi0y, __dmul_rn(double(w.Y), g.dphiy));
       const double2 sc = cphase_d(__dadd_rn(phx, phy));
@@ -501,42 +529,42 @@ __device__ __forceinline__ void grid_cells(
                            g.pos_w ? -__double2float_rn(sc.y)
                                    : __double2float_rn(sc.y));
     }
-    const int idx = w.Y * R + w.X;
     if constexpr (!MIXED) {
       double sx = 0.0, sy = 0.0;
 #pragma unroll
       for (int v = 0; v < N; ++v) {
         if (DENSE || pp[v] >= 0) {
-          const float2 cf = cfv[v][c];
-          const float2 prod = g.screen_on ? cmul_f(cmul_f(cf, screen), gv[v])
-                                          : cmul_f(cf, gv[v]);
+          const float2 cf = ptx::lds_f2(ca + po[v]);
+          const float2 prod = SCREEN ? cmul_f(cmul_f(cf, screen), gv[v])
+                                     : cmul_f(cf, gv[v]);
           sx = __dadd_rn(sx, double(prod.x));
           sy = __dadd_rn(sy, double(prod.y));
         }
       }
-      double2 t = gbase[idx];
+      double2 t = ptx::lds_d2(w.tile);
       t.x += sx;
       t.y = g.pos_w ? t.y - sy : t.y + sy;
-      gbase[idx] = t;
+      ptx::sts_d2(w.tile, t);
     } else {
       float sx = 0.f, sy = 0.f;
 #pragma unroll
       for (int v = 0; v < N; ++v) {
         if (DENSE || pp[v] >= 0) {
-          float2 cf = cfv[v][c];
-          if (g.screen_on)
+          float2 cf = ptx::lds_f2(ca + po[v]);
+          if constexpr (SCREEN)
             cf = make_float2(cf.x * screen.x - cf.y * screen.y,
                              cf.x * screen.y + cf.y * screen.x);
           sx = fmaf(cf.x, gv[v].x, fmaf(-cf.y, gv[v].y, sx));
           sy = fmaf(cf.x, gv[v].y, fmaf(cf.y, gv[v].x, sy));
         }
       }
-      float2 t = gbase[idx];
+      float2 t = ptx::lds_f2(w.tile);
       t.x += sx;
       t.y = g.pos_w ? t.y - sy : t.y + sy;
-      gbase[idx] = t;
+      ptx::sts_f2(w.tile, t);
     }
     w.next(tx);
+    ca += dca;
   }
 }
 
@@ -582,7 +610,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
   const bool exchange = p.do_degrid && p.has_model;
   // every role that reads a ring slot releases it (one exchange warp per
   // visibility)
-  const uint32_t empty_count = uint32_t((exchange ? kDG : 0) + 1 + kGR);
+  const uint32_t empty_count = uint32_t((exchange ? kDGPer : 0) + 1 + kGR);
 
   if (tid == 0) {
     for (int s = 0; s < kSlots; ++s) {
@@ -592,7 +620,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
     ptx::mbar_init(model_bar, 1);
     for (int x = 0; x < kXSlots; ++x) ptx::mbar_init(&xchg[x], 1);
     for (int x = 0; x < 2; ++x) {
-      ptx::mbar_init(&dgfull[x], kDG);
+      ptx::mbar_init(&dgfull[x], kDGPer);
       ptx::mbar_init(&dgempty[x], 1);
     }
     for (int x = 0; x < kSlots; ++x) ptx::mbar_init(&gvfull[x], 1);
@@ -619,12 +647,22 @@ tiled_kernel(const __grid_constant__ TiledParams p,
 
   if (warp == kPWarp) {
     // ---------------- producer warp ----------------
-    // Lane k holds the slice references of visibilities base+k and
-    // base+32+k of the current chunk; per visibility the warp reserves a
-    // descriptor slot and room in the byte ring, and lane 0 issues the bulk
-    // copies of its descriptor and of the CF planes of this CTA's row and
-    // pulls the slice of the visibility kPrefetch places ahead into L2.
-    constexpr int kPrefetch = 16;  // < 32, so the window cur/nxt covers it
+    // Lane k holds the slice reference of visibility base+k of the current
+    // chunk; per visibility the warp reserves a descriptor slot and room in
+    // the byte ring, and lane 0 issues the bulk copies of its descriptor and
+    // of the CF planes of this CTA's row.  (An L2 prefetch of later slices
+    // was measured to slow the kernel: the ring already keeps enough copies
+    // in flight to cover the HBM latency.)
+    // this row's plane runs, held in registers (loops below are unrolled)
+    const int nruns = p.nruns[row];
+    const int nplanes = p.nplanes[row];
+    int run_plane[kMaxRuns], run_len[kMaxRuns], run_dst[kMaxRuns];
+#pragma unroll
+    for (int u = 0; u < kMaxRuns; ++u) {
+      run_plane[u] = p.run_plane[row][u];
+      run_len[u] = p.run_len[row][u];
+      run_dst[u] = p.run_dst[row][u];
+    }
     uint32_t q = 0;
     uint32_t q_old = 0;               // oldest visibility not yet reclaimed
     unsigned long long head = 0;      // ring bytes allocated (monotonic)
@@ -633,29 +671,21 @@ tiled_kernel(const __grid_constant__ TiledParams p,
     TT_DECL(2);
     for (unsigned c = cid; c < nchunks; c += ncl) {
       const Chunk ch = p.chunks[c];
-      SliceRef cur{}, nxt{};
-      if (lane < ch.count) cur = p.srefs[ch.start + lane];
-      if (32 + lane < ch.count) nxt = p.srefs[ch.start + 32 + lane];
+      SliceRef cur{};
       for (int k = 0; k < ch.count; ++k, ++q) {
-        if (k > 0 && (k & 31) == 0) {
-          cur = nxt;
-          nxt = SliceRef{};
-          if (k + 32 + lane < ch.count) nxt = p.srefs[ch.start + k + 32 + lane];
+        if ((k & 31) == 0) {
+          cur = SliceRef{};
+          if (k + lane < ch.count) cur = p.srefs[ch.start + k + lane];
         }
         const int kk = k & 31;
         const long long off = __shfl_sync(0xffffffffu, cur.off, kk);
         const int pstride = __shfl_sync(0xffffffffu, cur.pstride, kk);
-        const int kp = kk + kPrefetch;  // < 64
-        const long long poff = kp < 32 ? __shfl_sync(0xffffffffu, cur.off, kp & 31)
-                                       : __shfl_sync(0xffffffffu, nxt.off, kp & 31);
-        const int ppst = kp < 32 ? __shfl_sync(0xffffffffu, cur.pstride, kp & 31)
-                                 : __shfl_sync(0xffffffffu, nxt.pstride, kp & 31);
         // Reclaim the oldest visibilities' slots until a descriptor slot
         // is free and the CF part fits in the byte ring (allocations never
         // straddle the ring end; they are released in order).
         const bool cf_needed = exchange || p.do_grid;
         const uint32_t pbytes = uint32_t(pstride) * 8u;
-        const uint32_t need = cf_needed ? uint32_t(p.nplanes[row]) * pbytes : 0u;
+        const uint32_t need = cf_needed ? uint32_t(nplanes) * pbytes : 0u;
         const uint32_t rb = uint32_t(p.ring_bytes);
         TT_BEGIN();
         for (;;) {
@@ -695,17 +725,12 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           if (cf_needed) {
             unsigned char* dst = ring + roff;
             const float2* slice = p.cf + off;
-            for (int u = 0; u < p.nruns[row]; ++u)
-              ptx::bulk_g2s(dst + p.run_dst[row][u] * pbytes,
-                            slice + size_t(p.run_plane[row][u]) * pstride,
-                            uint32_t(p.run_len[row][u]) * pbytes, &full[s]);
-            if (k + kPrefetch < ch.count) {
-              const float2* sl = p.cf + poff;
-              const uint32_t pb = uint32_t(ppst) * 8u;
-              for (int u = 0; u < p.nruns[row]; ++u)
-                ptx::bulk_prefetch_l2(sl + size_t(p.run_plane[row][u]) * ppst,
-                                      uint32_t(p.run_len[row][u]) * pb);
-            }
+#pragma unroll
+            for (int u = 0; u < kMaxRuns; ++u)
+              if (u < nruns)
+                ptx::bulk_g2s(dst + run_dst[u] * pbytes,
+                              slice + size_t(run_plane[u]) * pstride,
+                              uint32_t(run_len[u]) * pbytes, &full[s]);
           }
           TT_END(1);
         }
@@ -756,9 +781,10 @@ tiled_kernel(const __grid_constant__ TiledParams p,
 
       if (warp < kDG) {
         // -------- degridding warps --------
+        const int grp = warp / kDGPer;
         for (int k = 0; k < ch.count; ++k, ++q) {
           const int s = int(q % uint32_t(kSlots));
-          if (!exchange) continue;
+          if (!exchange || int(q % kDGGroups) != grp) continue;
           TT_BEGIN();
           ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
           TT_END(1);
@@ -773,9 +799,18 @@ tiled_kernel(const __grid_constant__ TiledParams p,
 #pragma unroll
             for (int v = 0; v < N; ++v)
               pp[v] = int(int8_t((vg.pos_w ? dpk[1] : dpk[0]) >> (8 * v)));
-            degrid_cells<N, MIXED, DENSE>(
-                vg, pp, reinterpret_cast<const float2*>(ring + ring_off[s]),
-                mtile, R, warp * 32 + lane, kDG * 32, acc);
+            // the phase screen is a separate instantiation: its code in
+            // the loop costs instructions even when it is skipped
+            if (vg.screen_on)
+              degrid_cells<N, MIXED, DENSE, true>(
+                  vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]),
+                  ptx::smem(mtile), R, (warp % kDGPer) * 32 + lane,
+                  kDGPer * 32, acc);
+            else
+              degrid_cells<N, MIXED, DENSE, false>(
+                  vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]),
+                  ptx::smem(mtile), R, (warp % kDGPer) * 32 + lane,
+                  kDGPer * 32, acc);
           }
           // warp sum of the 8 (padded) partials: halve the values held per
           // lane at each of the first three levels, then butterfly; lane
@@ -852,7 +887,8 @@ tiled_kernel(const __grid_constant__ TiledParams p,
               const bool live = !ptx::warp_flag(abort);
               double tot = 0.0;
               if (live && lane < 2 * N)
-                for (int w = 0; w < kDG; ++w) tot += dgpart[(b * kDG + w) * 8 + lane];
+                for (int w = b * kDGPer; w < (b + 1) * kDGPer; ++w)
+                  tot += dgpart[(b * kDG + w) * 8 + lane];
               __syncwarp();
               if (live && lane == 0) {
                 ptx::mbar_arrive(&dgempty[b]);
@@ -954,9 +990,14 @@ tiled_kernel(const __grid_constant__ TiledParams p,
                 gv[v] = gvring[gs * 4 + v];
                 if (vg.pos_w) gv[v].y = -gv[v].y;
               }
-              grid_cells<N, MIXED, DENSE>(
-                  vg, pp, reinterpret_cast<const float2*>(ring + ring_off[s]),
-                  gv, gtile, R, gw * 32 + lane, kGR * 32);
+              if (vg.screen_on)
+                grid_cells<N, MIXED, DENSE, true>(
+                    vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]), gv,
+                    ptx::smem(gtile), R, gw * 32 + lane, kGR * 32);
+              else
+                grid_cells<N, MIXED, DENSE, false>(
+                    vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]), gv,
+                    ptx::smem(gtile), R, gw * 32 + lane, kGR * 32);
             }
             TT_END(7);
           }
@@ -1027,7 +1068,8 @@ struct Plan {
   int smem = 0;
 };
 
-Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed) {
+Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
+               size_t nvis) {
   Plan pl;
   const CFRegion& cf = g->cf;
   const int nrow = int(g->grid_size[2]);
@@ -1098,9 +1140,26 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed) {
   const int eg = do_grid ? esize : 0;
   const int budget = 227 * 1024;
   const int taps = std::max(cf.max_taps_x, cf.max_taps_y);
-  // CF byte ring: about four of the largest parts (more in flight when
-  // parts are smaller), at least two; the tiles take the rest
-  for (int m = 4; m >= 2; --m) {
+  // CF byte ring: five of the largest parts if the tiles still fit, else
+  // four (more visibilities in flight when parts are smaller); the tiles
+  // take the rest.  Four is the least that cannot deadlock: an exchange warp
+  // releases visibility q only after visibility q + 2 has arrived, so the
+  // ring must take a third part while it holds any two, and an allocation
+  // that does not fit before the ring end starts over at its beginning.
+  // The deeper ring is taken only while the smaller tiles it leaves still
+  // hold kMinVisPerTile visibilities of the batch on average (measured: the
+  // deeper ring wins at 10M visibilities on a 2048^2 grid in both forms,
+  // loses at 1M in the FP64 form, whose 16-byte tiles shrink to 5x5 cells).
+  constexpr int kMinRingParts = 4;
+  constexpr size_t kMinVisPerTile = 32;
+  const bool fixed = g->tiled_ring_parts > 0;
+  const int m_hi = fixed ? g->tiled_ring_parts : 5;
+  const int m_lo = fixed ? g->tiled_ring_parts : kMinRingParts;
+  if (m_lo < kMinRingParts) {
+    pl.why = "the CF ring must hold at least four parts";
+    return pl;
+  }
+  for (int m = m_hi; m >= m_lo; --m) {
     const int rb = m * part;
     const SmemLayout L0 = smem_layout(rb, 0, em, eg);
     const int left = budget - L0.total - 1024 - 1024;
@@ -1108,6 +1167,12 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed) {
     int R = (em + eg) > 0 ? int(std::sqrt(double(left) / double(em + eg))) : 128;
     R = std::min(R, 128) & ~1;
     if (R - taps + 1 < 4) continue;
+    if (!fixed && m > m_lo) {
+      const size_t T = size_t(R - taps + 1);
+      const size_t ntiles = ((g->grid_size[0] + T - 1) / T) *
+                            ((g->grid_size[1] + T - 1) / T) * g->grid_size[3];
+      if (nvis < kMinVisPerTile * ntiles) continue;
+    }
     pl.ring_bytes = rb;
     pl.R = R;
     break;
@@ -1117,7 +1182,8 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed) {
     return pl;
   }
   pl.T = pl.R - taps + 1;
-  pl.K = mixed ? kChunkVisMixed : kChunkVisFP64;
+  pl.K = g->tiled_chunk_vis > 0 ? g->tiled_chunk_vis
+                                : (mixed ? kChunkVisMixed : kChunkVisFP64);
   pl.smem = smem_layout(pl.ring_bytes, pl.R, em, eg).total + 1024;
   if (em > 0 && (2 * size_t(g->grid_size[0]) * (mixed ? 4 : 8)) % 16 != 0) {
     pl.why = "model row pitch not a 16-byte multiple";
@@ -1350,7 +1416,7 @@ Status grid_tiled(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
   }
   if (n > size_t(0x7fffffff)) return Status::ok();
   const bool mixed = g->precision == HPGB_PRECISION_MIXED;
-  const Plan plan = make_plan(g, flags, mixed);
+  const Plan plan = make_plan(g, flags, mixed, n);
   if (!plan.ok) return Status::ok();
   *used = true;
   switch (g->npol) {

@@ -1,15 +1,12 @@
 // ptx.cuh -- thin wrappers over the sm_90+/sm_100a PTX used by the tiled
 // kernel: mbarriers (with bounded waits), bulk and tensor TMA copies into
-// shared memory, L2 bulk prefetch and distributed-shared-memory access within
-// a thread-block cluster.  No multicast form is used anywhere.
+// shared memory, shared-memory loads and stores at 32-bit addresses and
+// distributed-shared-memory access within a thread-block cluster.  No
+// multicast form is used anywhere.
 #pragma once
 
 #include <cuda.h>
 #include <stdint.h>
-
-#ifndef WAIT_MAX_SLEEP_NS
-#define WAIT_MAX_SLEEP_NS 256
-#endif
 
 namespace hpgb {
 namespace ptx {
@@ -56,13 +53,20 @@ __device__ __forceinline__ void mbar_arrive_remote(uint64_t* bar,
 }
 
 // Waits for the completion of the mbarrier phase with the given parity.
-// Every lane of the calling warp polls (try_wait), so the warp stays
-// converged; between polls the warp backs off with __nanosleep (doubling up
-// to kMaxSleepNs) so that waiting warps leave issue slots to working ones.
-// After kMaxTries polls (under a second) the wait gives up and returns
-// false, and the caller records the timeout instead of hanging.
-constexpr uint32_t kMaxTries = 1u << 21;
-constexpr uint32_t kMaxSleepNs = WAIT_MAX_SLEEP_NS;
+// Every lane of the calling warp waits (the warp stays converged).  After a
+// first plain test, each try_wait carries a suspend-time hint, so the warp
+// sleeps in hardware until the phase completes (or the hint runs out)
+// instead of spinning.  The wait is bounded by the global timer: after
+// kWaitLimitNs it sets the CTA-wide abort flag and returns false, and the
+// caller records the timeout instead of hanging.
+constexpr uint32_t kSuspendHintNs = 20000;
+constexpr uint64_t kWaitLimitNs = 500000000ull;  // 0.5 s
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
   uint32_t done;
@@ -71,6 +75,17 @@ __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
       "selp.u32 %0, 1, 0, p; }"
       : "=r"(done)
       : "r"(a), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ bool mbar_try_suspend(uint32_t a, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, "
+      "%3; selp.u32 %0, 1, 0, p; }"
+      : "=r"(done)
+      : "r"(a), "r"(parity), "r"(kSuspendHintNs)
       : "memory");
   return done != 0;
 }
@@ -86,20 +101,30 @@ __device__ __forceinline__ bool mbar_try_cluster(uint32_t a, uint32_t parity) {
   return done != 0;
 }
 
+__device__ __forceinline__ bool mbar_try_cluster_suspend(uint32_t a,
+                                                         uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.acquire.cluster.shared::cta."
+      "b64 p, [%1], %2, %3; selp.u32 %0, 1, 0, p; }"
+      : "=r"(done)
+      : "r"(a), "r"(parity), "r"(kSuspendHintNs)
+      : "memory");
+  return done != 0;
+}
+
 // `abort` is a CTA-wide shared-memory flag: a wait that gives up sets it,
 // and every later wait returns false at once, so a broken pipeline ends
 // quickly with an error status instead of timing out wait after wait.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
                                           volatile int* abort) {
   const uint32_t a = smem(bar);
-  uint32_t ns = 16;
-  for (uint32_t i = 0; i < kMaxTries; ++i) {
-    if (mbar_try(a, parity)) return true;
+  if (mbar_try(a, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    if (mbar_try_suspend(a, parity)) return true;
     if (*abort) return false;
-    if (kMaxSleepNs) {
-      __nanosleep(ns);
-      ns = ns < kMaxSleepNs ? ns * 2 : kMaxSleepNs;
-    }
+    if (global_ns() - t0 > kWaitLimitNs) break;
   }
   *abort = 1;
   return false;
@@ -110,14 +135,12 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar,
                                                   uint32_t parity,
                                                   volatile int* abort) {
   const uint32_t a = smem(bar);
-  uint32_t ns = 16;
-  for (uint32_t i = 0; i < kMaxTries; ++i) {
-    if (mbar_try_cluster(a, parity)) return true;
+  if (mbar_try_cluster(a, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    if (mbar_try_cluster_suspend(a, parity)) return true;
     if (*abort) return false;
-    if (kMaxSleepNs) {
-      __nanosleep(ns);
-      ns = ns < kMaxSleepNs ? ns * 2 : kMaxSleepNs;
-    }
+    if (global_ns() - t0 > kWaitLimitNs) break;
   }
   *abort = 1;
   return false;
@@ -128,6 +151,34 @@ __device__ __forceinline__ bool warp_flag(volatile int* flag) {
   return __shfl_sync(0xffffffffu, *flag, 0) != 0;
 }
 
+// shared-memory loads and stores at 32-bit shared-window addresses
+__device__ __forceinline__ float2 lds_f2(uint32_t a) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];"
+               : "=f"(v.x), "=f"(v.y)
+               : "r"(a));
+  return v;
+}
+
+__device__ __forceinline__ double2 lds_d2(uint32_t a) {
+  double2 v;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];"
+               : "=d"(v.x), "=d"(v.y)
+               : "r"(a));
+  return v;
+}
+
+__device__ __forceinline__ void sts_f2(uint32_t a, float2 v) {
+  asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.x),
+               "f"(v.y));
+}
+
+__device__ __forceinline__ void sts_d2(uint32_t a, double2 v) {
+  asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(a), "d"(v.x),
+               "d"(v.y));
+}
+
+
 // bulk copy global -> this CTA's shared memory, completion counted in bytes
 // on bar; dst, src and bytes are 16-byte multiples
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src,
@@ -137,13 +188,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src,
       "[%1], %2, [%3];" ::"r"(smem(dst)),
       "l"(src), "r"(bytes), "r"(smem(bar))
       : "memory");
-}
-
-__device__ __forceinline__ void bulk_prefetch_l2(const void* src,
-                                                 uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src),
-               "r"(bytes)
-               : "memory");
 }
 
 // 3-D tiled tensor load (no multicast); c0 is the innermost coordinate

@@ -332,6 +332,12 @@ class Gridder:
     def shift_model(self, direction=abi.SHIFT_FORWARD):
         check(load().hpgb_shift_model(self._h, int(direction)))
 
+    def set_tiled_plan(self, ring_parts=0, chunk_vis=0):
+        """Override the tiled kernel's ring depth (in largest CF parts) and
+        visibilities per tile pass; 0 keeps the automatic choice."""
+        check(load().hpgb_set_tiled_plan(self._h, int(ring_parts),
+                                         int(chunk_vis)))
+
     def profile_tiled_kernel(self, enable=True):
         """Record CUDA events around every tiled-kernel launch (benchmark
         instrumentation)."""

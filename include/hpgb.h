@@ -297,6 +297,15 @@ HPGB_API int hpgb_shift_model(hpgb_gridder* gridder, int direction);
 HPGB_API int hpgb_kernel_launches(const hpgb_gridder* gridder,
                                   uint64_t* count);
 
+/* Tiled-kernel plan overrides, no counterpart in the reference (tuning):
+ * ring_parts = number of the largest per-row CF parts the shared-memory
+ * ring holds (0 or 4..16; the tile side shrinks to make room), chunk_vis = visibilities
+ * per tile pass between flushes of the shared-memory grid tile; 0 keeps the
+ * plan's own choice.  A plan that does not fit makes the tiled kernel
+ * unusable for the batch (HPGB_KERNEL_AUTO then uses the direct kernels). */
+HPGB_API int hpgb_set_tiled_plan(hpgb_gridder* gridder, int ring_parts,
+                                 int chunk_vis);
+
 /* Benchmark instrumentation, no counterpart in the reference: while
  * enabled, CUDA events are recorded on the gridder's stream around every
  * launch of the tiled gridding kernel.  hpgb_tiled_kernel_time waits for the

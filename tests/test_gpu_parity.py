@@ -200,6 +200,38 @@ def test_degrid_grid_parity(gpu, oracle_lib, grad, kernel, precision):
     np.testing.assert_allclose(g.grid_weights(), o.weights, rtol=1e-12)
 
 
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED],
+                         ids=["fp64", "mixed"])
+@pytest.mark.parametrize("ring_parts,chunk", [(4, 64), (6, 0), (5, 7)])
+def test_tiled_plan_overrides(gpu, oracle_lib, precision, ring_parts, chunk):
+    """Every ring depth and tile-pass length the plan accepts gives the same
+    results: small chunks cross many tile flushes, a deep ring keeps many
+    visibilities in flight."""
+    cfg = small_full_pol(3000, grad=0.4)
+    g, o = make_pair(cfg, oracle_lib, precision=precision, kernel="tiled")
+    g.set_tiled_plan(ring_parts, chunk)
+    fut = g.degrid_grid_get_residual_visibilities(cfg["vis"])
+    g.fence()
+    exp = o.grid_visibilities(cfg["vis"], do_degrid=True, return_vis=True)
+    res = fut.get()
+    if precision == abi.PRECISION_FP64:
+        assert np.mean(np.all(res["vis"] == exp["vis"], axis=1)) > 0.99
+    else:
+        assert rel_norm(res["vis"], exp["vis"]) <= 1e-6
+    assert rel_norm(g.grid_values(), o.grid) <= 1e-6
+    np.testing.assert_allclose(g.grid_weights(), o.weights, rtol=1e-12)
+
+
+def test_tiled_plan_rejects_shallow_ring(gpu, oracle_lib):
+    """A ring of fewer than four parts could stall the pipeline: refused."""
+    cfg = small_full_pol(10)
+    g, _ = make_pair(cfg, oracle_lib, kernel="tiled")
+    for bad in ((3, 0), (2, 0), (17, 0), (0, -1)):
+        with pytest.raises(HpgError):
+            g.set_tiled_plan(*bad)
+    g.set_tiled_plan(0, 0)
+
+
 @pytest.mark.parametrize("kernel,precision", KERNELS, ids=KERNEL_IDS)
 def test_degrid_grid_no_model(gpu, oracle_lib, kernel, precision):
     """Without a model the residual is the input (src/hpg_core.hpp:614)."""
