@@ -499,7 +499,8 @@ __device__ __forceinline__ void degrid_cells(
 // Gridding of one visibility's footprint cells c = first, first + stride,
 // ... into the row's shared-memory grid tile (src/hpg_core.hpp:856-873).
 // The gridding warps cover every cell of one visibility between two
-// barriers, so no two threads add to a tile cell at once.  pp[v]: slot
+// barriers, so no two threads add to a tile cell at once (measured faster
+// than shared-memory atomics with two visibilities in flight).  pp[v]: slot
 // plane of Mueller element gmi[row][v] (-1 if inactive; never when DENSE).
 // gv[v] arrive conjugated when w > 0 (the CF imaginary part is negated
 // then): conj(cf)*s*g = conj(cf*conj(s)*conj(g)), bit for bit in the
@@ -910,6 +911,16 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             const TileDesc& d = descs[prev_s];
             const int xs = int(qq % uint32_t(kXSlots));
             const int gs = int(qq % uint32_t(kSlots));
+            // everything the finish needs from the descriptor is read
+            // before the wait, so only the partial sums remain after it
+            const int v = lane < N ? lane : 0;
+            const double2 wfac = d.wfac[v];
+            const float2 val = d.vals[v];
+            const float wgt = d.weights[v];
+            const double2 phasor = d.phasor;
+            const float2 gv0 = d.gvis[v];
+            const int vis_index = d.index;
+            const double twgt = d.twgt[row];
             if (exchange)
               ok &= ptx::mbar_wait_cluster(&xchg[xs], (qq / kXSlots) & 1, abort);
             TT_END(3);
@@ -917,36 +928,42 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             const bool live = !ptx::warp_flag(abort);
             float2 gout = make_float2(0.f, 0.f);
             if (live && lane < N) {
-              const int v = lane;
               if (p.do_degrid) {
                 float2 pred = make_float2(0.f, 0.f);
                 if (exchange) {
+                  const double2* x =
+                      reinterpret_cast<const double2*>(xbuf) + (xs * 4) * 4 + v;
+                  double2 part[4];
+#pragma unroll
+                  for (int r = 0; r < 4; ++r)
+                    part[r] = r < p.nrow ? x[r * 4] : make_double2(0.0, 0.0);
                   double2 num = make_double2(0.0, 0.0);
-                  for (int r = 0; r < p.nrow; ++r) {
-                    const double* x = &xbuf[((xs * 4 + r) * 4 + v) * 2];
-                    num.x += x[0];
-                    num.y += x[1];
-                  }
-                  const double2 qv = cmul_d(num, d.wfac[v]);
+#pragma unroll
+                  for (int r = 0; r < 4; ++r)
+                    if (r < p.nrow) {
+                      num.x += part[r].x;
+                      num.y += part[r].y;
+                    }
+                  const double2 qv = cmul_d(num, wfac);
                   pred = make_float2(__double2float_rn(qv.x),
                                      __double2float_rn(qv.y));
                 }
                 float2* out = reinterpret_cast<float2*>(
-                    p.records + size_t(d.index) * p.rec_stride);
+                    p.records + size_t(vis_index) * p.rec_stride);
                 if (p.do_grid) {
-                  const float2 rr = make_float2(__fsub_rn(d.vals[v].x, pred.x),
-                                                __fsub_rn(d.vals[v].y, pred.y));
+                  const float2 rr = make_float2(__fsub_rn(val.x, pred.x),
+                                                __fsub_rn(val.y, pred.y));
                   if (row == 0) out[v] = rr;
-                  gout = scale_for_gridding(rr, d.phasor, d.weights[v]);
+                  gout = scale_for_gridding(rr, phasor, wgt);
                 } else if (row == 0) {
                   out[v] = pred;
                 }
               } else {
-                gout = d.gvis[v];
+                gout = gv0;
               }
               if (p.do_grid) gvring[gs * 4 + v] = gout;
             }
-            if (live && lane == 0 && p.do_grid) wchunk += d.twgt[row];
+            if (live && lane == 0 && p.do_grid) wchunk += twgt;
             __syncwarp();
             if (live && lane == 0) {
               if (p.do_grid) ptx::mbar_arrive(&gvfull[gs]);
