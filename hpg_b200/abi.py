@@ -115,6 +115,10 @@ SIGNATURES = {
     "hpgb_set_model": ([_P, _P, _P, _I, _I], _I),
     "hpgb_grid_visibilities": ([_P, _P, _S, _U, _U, _I, _P], _I),
     "hpgb_grid_visibilities_noalloc": ([_P, _P, _S, _U, _U], _I),
+    "hpgb_degrid_linear": ([_P, _P, _S, _U, _P, _P], _I),
+    "hpgb_degrid_adjoint": ([_P, _P, _S, _U, _P, _P], _I),
+    "hpgb_grid_linear": ([_P, _P, _S, _U, _P, _P], _I),
+    "hpgb_grid_adjoint": ([_P, _P, _S, _U, _P, _P], _I),
     "hpgb_fence": ([_P], _I),
     "hpgb_copy_weights": ([_P, _P, _I], _I),
     "hpgb_copy_grid": ([_P, _P, _I], _I),

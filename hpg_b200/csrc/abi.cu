@@ -465,6 +465,49 @@ int hpgb_grid_visibilities_noalloc(hpgb_gridder* g, void* vis, size_t n,
   });
 }
 
+static int linear_entry(hpgb_gridder* g, const void* vis, size_t n,
+                        unsigned npol, int op, const void* in, void* out) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    if (n > g->max_batch)
+      return Status::err(HPGB_ERROR_EXCESSIVE_NUMBER_VISIBILITIES,
+                         "Number of visibilities exceeds maximum batch size");
+    if (npol != g->npol)
+      return Status::err(HPGB_ERROR_INVALID_NUMBER_POLARIZATIONS,
+                         "Number of visibility polarizations does not match "
+                         "Mueller matrix");
+    if (n == 0) return Status::ok();
+    if (!vis || !in || !out) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    if (!g->cf.set)
+      return Status::err(HPGB_ERROR_OTHER, "no convolution function set");
+    HPGB_TRY(validate_mueller(g));
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    return linear_op(g, vis, n, op, in, out);
+  });
+}
+
+int hpgb_degrid_linear(hpgb_gridder* g, const void* vis, size_t n,
+                       unsigned npol, const void* model, void* values) {
+  return linear_entry(g, vis, n, npol, 0, model, values);
+}
+
+int hpgb_degrid_adjoint(hpgb_gridder* g, const void* vis, size_t n,
+                        unsigned npol, const void* values_cotangent,
+                        void* model_cotangent) {
+  return linear_entry(g, vis, n, npol, 1, values_cotangent, model_cotangent);
+}
+
+int hpgb_grid_linear(hpgb_gridder* g, const void* vis, size_t n,
+                     unsigned npol, const void* values, void* grid) {
+  return linear_entry(g, vis, n, npol, 2, values, grid);
+}
+
+int hpgb_grid_adjoint(hpgb_gridder* g, const void* vis, size_t n,
+                      unsigned npol, const void* grid_cotangent,
+                      void* values_cotangent) {
+  return linear_entry(g, vis, n, npol, 3, grid_cotangent, values_cotangent);
+}
+
 int hpgb_fence(const hpgb_gridder* g) {
   return guarded([&]() -> Status {
     if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");

@@ -126,6 +126,13 @@ Status grid_direct_noalloc(hpgb_gridder* g, void* d_vis, size_t n,
 Status debug_coords(hpgb_gridder* g, const void* d_vis, size_t n,
                     hpgb_vis_coords* d_out);
 
+// adjoint.cu: FP64 linear operators on device arrays; op 0 = degridding D
+// (model -> values), 1 = its adjoint (values -> model, accumulated),
+// 2 = gridding G (values -> grid, accumulated), 3 = its adjoint (grid ->
+// values)
+Status linear_op(hpgb_gridder* g, const void* d_vis, size_t n, int op,
+                 const void* in, void* out);
+
 // imaging.cu
 Status normalize_by_weights(hpgb_gridder* g, double wfactor);
 Status scale_grid(hpgb_gridder* g, double2* grid, double norm);

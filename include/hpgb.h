@@ -252,6 +252,45 @@ HPGB_API int hpgb_grid_visibilities_noalloc(hpgb_gridder* gridder,
                                             unsigned num_polarizations,
                                             unsigned flags);
 
+/* Differentiable imaging: the degridding and gridding maps as FP64 linear
+ * operators and their adjoints (no counterpart in the reference's State;
+ * the maps are those of src/hpg_core.hpp:580-682 and :791-886).
+ * visibilities: num_visibilities hpgb_visdataN records in device memory;
+ * only their geometry is read (uvw, freq, phase, weights, grid_cube,
+ * cf_index, cf_phase_gradient), never their vis values.  Grid-shaped
+ * arrays are complex<double> in the gridder's device grid layout
+ * [cube][mrow][y][x] (as hpgb_grid_device_ptr); per-visibility arrays are
+ * complex<double> [num_visibilities][num_polarizations].  All arrays are in
+ * device memory; the work is queued on the gridder's stream (hpgb_fence
+ * waits for it).  Visibilities outside the grid contribute nothing.
+ *
+ * hpgb_degrid_linear:  values = D model, the degridding prediction
+ *   conj(phasor) / normaliser * sum cf * screen* * model, in FP64 without
+ *   rounding to complex<float> (overwrites values).
+ * hpgb_degrid_adjoint: model_cotangent += D^H values_cotangent.
+ * hpgb_grid_linear:    grid += G values, gridding of phasor * weight * values
+ *   with FP64 products.
+ * hpgb_grid_adjoint:   values_cotangent = G^H grid_cotangent (overwrites). */
+HPGB_API int hpgb_degrid_linear(hpgb_gridder* gridder, const void* visibilities,
+                                size_t num_visibilities,
+                                unsigned num_polarizations, const void* model,
+                                void* values);
+HPGB_API int hpgb_degrid_adjoint(hpgb_gridder* gridder,
+                                 const void* visibilities,
+                                 size_t num_visibilities,
+                                 unsigned num_polarizations,
+                                 const void* values_cotangent,
+                                 void* model_cotangent);
+HPGB_API int hpgb_grid_linear(hpgb_gridder* gridder, const void* visibilities,
+                              size_t num_visibilities,
+                              unsigned num_polarizations, const void* values,
+                              void* grid);
+HPGB_API int hpgb_grid_adjoint(hpgb_gridder* gridder, const void* visibilities,
+                               size_t num_visibilities,
+                               unsigned num_polarizations,
+                               const void* grid_cotangent,
+                               void* values_cotangent);
+
 /* State::fence (src/hpg_runtime.hpp:153-154). */
 HPGB_API int hpgb_fence(const hpgb_gridder* gridder);
 

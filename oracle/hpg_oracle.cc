@@ -427,6 +427,41 @@ void grid_visibilities(const oracle_params& p, VisData<N>* vis, size_t n,
     std::memcpy(static_cast<void*>(vis), work.data(), n * sizeof(VisData<N>));
 }
 
+// Degridding normaliser of each visibility polarization, the den of
+// degrid_vis (src/hpg_core.hpp:598-600, :659-661): the sum over grid rows
+// and footprint of the degridding CF, 1 where that sum is 0 or the
+// visibility is off the grid.  out: complex<double> [n][N].
+template <int N>
+void normalisers(const oracle_params& p, const VisData<N>* vis, size_t n,
+                 double* out) {
+  for (size_t i = 0; i < n; ++i) {
+    cf32 vals[N];
+    const Vis<N> v = make_vis<N>(p, vis[i], vals);
+    c64 den[N];
+    for (int k = 0; k < N; ++k) den[k] = c64(0);
+    if (all_within_grid(v, p.grid_size)) {
+      const auto& mi = v.pos_w ? p.conj_mueller : p.mueller;
+      const float im_factor = v.pos_w ? 1.0f : -1.0f;
+      for (int gpol = 0; gpol < p.grid_size[2]; ++gpol)
+        for (int X = 0; X < v.cf_size[0]; ++X)
+          for (int Y = 0; Y < v.cf_size[1]; ++Y)
+            for (int k = 0; k < N; ++k) {
+              const int m = mi[gpol][k];
+              if (m >= 0) {
+                cf32 cfv = cf_at(p, v, X, Y, m);
+                cfv.imag(cfv.imag() * im_factor);
+                den[k] += c64(cfv.real(), cfv.imag());
+              }
+            }
+    }
+    for (int k = 0; k < N; ++k) {
+      const c64 d = den[k] != c64(0) ? den[k] : c64(1);
+      out[2 * (i * N + k)] = d.real();
+      out[2 * (i * N + k) + 1] = d.imag();
+    }
+  }
+}
+
 template <int N>
 void coords(const oracle_params& p, const VisData<N>* vis, size_t n,
             oracle_coords* out) {
@@ -463,6 +498,19 @@ int oracle_vis_coords(const oracle_params* p, const void* vis, size_t n,
     case 2: coords<2>(*p, static_cast<const VisData<2>*>(vis), n, out); break;
     case 3: coords<3>(*p, static_cast<const VisData<3>*>(vis), n, out); break;
     case 4: coords<4>(*p, static_cast<const VisData<4>*>(vis), n, out); break;
+    default: return -1;
+  }
+  return 0;
+}
+
+// Degridding normalisers, complex<double> [n][npol] (see normalisers()).
+int oracle_normalisers(const oracle_params* p, const void* vis, size_t n,
+                       int npol, double* out) {
+  switch (npol) {
+    case 1: normalisers<1>(*p, static_cast<const VisData<1>*>(vis), n, out); break;
+    case 2: normalisers<2>(*p, static_cast<const VisData<2>*>(vis), n, out); break;
+    case 3: normalisers<3>(*p, static_cast<const VisData<3>*>(vis), n, out); break;
+    case 4: normalisers<4>(*p, static_cast<const VisData<4>*>(vis), n, out); break;
     default: return -1;
   }
   return 0;

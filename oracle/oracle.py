@@ -69,6 +69,7 @@ def load():
         P = ctypes.c_void_p
         lib.oracle_num_threads.restype = ctypes.c_int
         lib.oracle_vis_coords.argtypes = [P, P, ctypes.c_size_t, ctypes.c_int, P]
+        lib.oracle_normalisers.argtypes = [P, P, ctypes.c_size_t, ctypes.c_int, P]
         lib.oracle_grid_visibilities.argtypes = [
             P, P, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_int,
             ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_int]
@@ -132,6 +133,16 @@ class Oracle:
         out = np.zeros(len(vis), COORDS_DTYPE)
         rc = load().oracle_vis_coords(ctypes.byref(self._p), _ptr(vis), len(vis),
                                       self.npol, _ptr(out))
+        assert rc == 0
+        return out
+
+    def normalisers(self, vis):
+        """Degridding normaliser per visibility polarization (reference
+        src/hpg_core.hpp:598-600, :659-661), complex128 [n][npol]."""
+        vis = np.ascontiguousarray(vis)
+        out = np.zeros((len(vis), self.npol), np.complex128)
+        rc = load().oracle_normalisers(ctypes.byref(self._p), _ptr(vis),
+                                       len(vis), self.npol, _ptr(out))
         assert rc == 0
         return out
 
