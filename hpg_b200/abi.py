@@ -135,6 +135,8 @@ SIGNATURES = {
     "hpgb_shift_model": ([_P, _I], _I),
     "hpgb_kernel_launches": ([_P, ctypes.POINTER(ctypes.c_uint64)], _I),
     "hpgb_set_tiled_plan": ([_P, _I, _I], _I),
+    "hpgb_autotune_tiled": ([_P, _P, _S, _U, _U, _I, ctypes.POINTER(_I),
+                             ctypes.POINTER(_I)], _I),
     "hpgb_profile_tiled_kernel": ([_P, _I], _I),
     "hpgb_tiled_kernel_time": ([_P, ctypes.POINTER(_D),
                                 ctypes.POINTER(ctypes.c_uint64)], _I),

@@ -679,6 +679,34 @@ int hpgb_set_tiled_plan(hpgb_gridder* g, int ring_parts, int chunk_vis) {
   });
 }
 
+int hpgb_autotune_tiled(hpgb_gridder* g, const void* vis, size_t n,
+                        unsigned npol, unsigned flags, int vis_on_device,
+                        int* ring_parts, int* chunk_vis) {
+  return guarded([&]() -> Status {
+    if (!g || !ring_parts || !chunk_vis)
+      return Status::err(HPGB_ERROR_OTHER, "null argument");
+    if (n > g->max_batch)
+      return Status::err(HPGB_ERROR_EXCESSIVE_NUMBER_VISIBILITIES,
+                         "Number of visibilities exceeds maximum batch size");
+    if (npol != g->npol)
+      return Status::err(HPGB_ERROR_INVALID_NUMBER_POLARIZATIONS,
+                         "Number of visibility polarizations does not match "
+                         "Mueller matrix");
+    if (!(flags & HPGB_DO_GRID) && (flags & HPGB_UPDATE_GRID_WEIGHTS))
+      return Status::err(HPGB_ERROR_UPDATE_WEIGHTS_WITHOUT_GRIDDING,
+                         "Unable to update grid weights during degridding only");
+    if (n == 0 || !vis)
+      return Status::err(HPGB_ERROR_OTHER, "autotuning needs visibilities");
+    if (!g->cf.set)
+      return Status::err(HPGB_ERROR_OTHER, "no convolution function set");
+    HPGB_TRY(validate_mueller(g));
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    HPGB_TRY(fence_impl(g));
+    return autotune_tiled(g, vis, n, flags & ~HPGB_RETURN_VISIBILITIES,
+                          vis_on_device != 0, ring_parts, chunk_vis);
+  });
+}
+
 int hpgb_profile_tiled_kernel(hpgb_gridder* g, int enable) {
   return guarded([&]() -> Status {
     if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");

@@ -115,6 +115,11 @@ Status copy_cf(hpgb_gridder* dst, const hpgb_gridder* src);
 Status grid_tiled(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
                   bool* used);
 
+// autotune.cu: times tiled plans on the batch, keeps the fastest
+Status autotune_tiled(hpgb_gridder* g, const void* vis, size_t n,
+                      unsigned flags, bool on_device, int* best_ring,
+                      int* best_chunk);
+
 // grid_direct.cu
 Status grid_direct(hpgb_gridder* g, const void* d_vis, size_t n,
                    unsigned flags);

@@ -338,6 +338,27 @@ class Gridder:
         check(load().hpgb_set_tiled_plan(self._h, int(ring_parts),
                                          int(chunk_vis)))
 
+    def autotune_tiled(self, visibilities, flags=None, on_device=False):
+        """Time the tiled kernel's candidate plans on this batch (grid and
+        weights are left unchanged) and keep the fastest; returns
+        (ring_parts, chunk_vis)."""
+        if flags is None:
+            flags = abi.DO_DEGRID | abi.DO_GRID | abi.UPDATE_GRID_WEIGHTS
+        ring = ctypes.c_int()
+        chunk = ctypes.c_int()
+        if on_device:
+            n = (visibilities.numel() * visibilities.element_size() //
+                 abi.visdata_dtype(self.npol).itemsize)
+        else:
+            visibilities = np.ascontiguousarray(visibilities)
+            n = len(visibilities)
+        check(load().hpgb_autotune_tiled(self._h, ptr(visibilities), n,
+                                         self.npol, int(flags),
+                                         int(bool(on_device)),
+                                         ctypes.byref(ring),
+                                         ctypes.byref(chunk)))
+        return ring.value, chunk.value
+
     def profile_tiled_kernel(self, enable=True):
         """Record CUDA events around every tiled-kernel launch (benchmark
         instrumentation)."""

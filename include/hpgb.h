@@ -345,6 +345,20 @@ HPGB_API int hpgb_kernel_launches(const hpgb_gridder* gridder,
 HPGB_API int hpgb_set_tiled_plan(hpgb_gridder* gridder, int ring_parts,
                                  int chunk_vis);
 
+/* Autotuner of the tiled kernel, no counterpart in the reference: runs the
+ * batch (as hpgb_grid_visibilities would with these flags) once per
+ * candidate plan -- CF ring depths 4..8, then tile-pass lengths around the
+ * fastest depth -- timing each with CUDA events, restores the grid and
+ * weights after every trial, and keeps the fastest plan for the gridder's
+ * later calls (as hpgb_set_tiled_plan would), returning it.  Synchronous.
+ * Costs about eight runs of the batch: tune on a representative batch once,
+ * then grid. */
+HPGB_API int hpgb_autotune_tiled(hpgb_gridder* gridder, const void* visibilities,
+                                 size_t num_visibilities,
+                                 unsigned num_polarizations, unsigned flags,
+                                 int vis_on_device, int* ring_parts,
+                                 int* chunk_vis);
+
 /* Benchmark instrumentation, no counterpart in the reference: while
  * enabled, CUDA events are recorded on the gridder's stream around every
  * launch of the tiled gridding kernel.  hpgb_tiled_kernel_time waits for the

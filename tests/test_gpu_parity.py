@@ -222,6 +222,32 @@ def test_tiled_plan_overrides(gpu, oracle_lib, precision, ring_parts, chunk):
     np.testing.assert_allclose(g.grid_weights(), o.weights, rtol=1e-12)
 
 
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED],
+                         ids=["fp64", "mixed"])
+def test_autotune_keeps_data_and_parity(gpu, oracle_lib, precision):
+    """The autotuner leaves grid and weights as they were and its chosen
+    plan gives the same results."""
+    cfg = small_full_pol(3000, grad=0.4, seed=9)
+    g, o = make_pair(cfg, oracle_lib, precision=precision, kernel="tiled")
+    first = cfg["vis"][:1000]
+    g.degrid_grid_visibilities(first)
+    o.grid_visibilities(first, do_degrid=True)
+    g.fence()
+    before = (g.grid_values(), g.grid_weights())
+    ring, chunk = g.autotune_tiled(cfg["vis"])
+    assert 4 <= ring <= 8 and chunk >= 0
+    assert np.array_equal(g.grid_values(), before[0])
+    assert np.array_equal(g.grid_weights(), before[1])
+    rest = cfg["vis"][1000:]
+    fut = g.degrid_grid_get_residual_visibilities(rest)
+    g.fence()
+    exp = o.grid_visibilities(rest, do_degrid=True, return_vis=True)
+    if precision == abi.PRECISION_FP64:
+        assert np.mean(np.all(fut.get()["vis"] == exp["vis"], axis=1)) > 0.99
+    assert rel_norm(g.grid_values(), o.grid) <= 1e-6
+    np.testing.assert_allclose(g.grid_weights(), o.weights, rtol=1e-12)
+
+
 def test_tiled_plan_rejects_shallow_ring(gpu, oracle_lib):
     """A ring of fewer than four parts could stall the pipeline: refused."""
     cfg = small_full_pol(10)
