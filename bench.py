@@ -56,6 +56,8 @@ def parse():
                         "for profiling captures; per-visibility work is "
                         "unchanged)")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-autotune", dest="autotune", action="store_false",
+                   help="skip the (untimed) autotuning of the tiled plan")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -330,10 +332,14 @@ def main():
     forms = (["mixed", "fp64"] if args.precision == "both"
              else [args.precision])
     results = {}
+    plans = {}
     clock_summary = None
     for form in forms:
         g.set_precision(hpg_b200.PRECISION_MIXED if form == "mixed"
                         else hpg_b200.PRECISION_FP64)
+        # untimed set-up: the autotuner picks the tiled plan on this batch
+        plan = g.autotune_tiled(dvis, on_device=True) if args.autotune else None
+        plans[form] = plan
         for _ in range(args.warmup):
             step_device()
         g.fence()
@@ -357,6 +363,8 @@ def main():
             "step_gbs": b_alg / (ms_step * 1e-3) / 1e9,
             "kernel_gbs": (b_kernel / (k_avg * 1e-3) / 1e9) if k_avg else None,
             "clocks": csum,
+            "tiled_plan": ({"ring_parts": plan[0], "chunk_vis": plan[1]}
+                           if plan else "automatic"),
         }
         if form == forms[0]:
             clock_summary = csum
@@ -366,6 +374,8 @@ def main():
     if not args.no_e2e:
         g.set_precision(hpg_b200.PRECISION_MIXED if forms[0] == "mixed"
                         else hpg_b200.PRECISION_FP64)
+        if plans.get(forms[0]):
+            g.set_tiled_plan(*plans[forms[0]])
         e2e_steps = max(1, min(args.steps, 3))
         step_e2e()
         ms_e2e = timed(step_e2e, e2e_steps)

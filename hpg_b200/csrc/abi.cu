@@ -10,6 +10,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "gridder.cuh"
@@ -107,7 +108,7 @@ Status validate_host_indexes(const hpgb_gridder* g, const void* vis, size_t n) {
   return Status::ok();
 }
 
-Status validate_indexes(const hpgb_gridder* g, const void* vis, size_t n) {
+Status validate_range(const hpgb_gridder* g, const void* vis, size_t n) {
   switch (g->npol) {
     case 1: return validate_host_indexes<1>(g, vis, n);
     case 2: return validate_host_indexes<2>(g, vis, n);
@@ -115,6 +116,41 @@ Status validate_indexes(const hpgb_gridder* g, const void* vis, size_t n) {
     case 4: return validate_host_indexes<4>(g, vis, n);
     default: return Status::err(HPGB_ERROR_OTHER, "bad polarization count");
   }
+}
+
+// large batches are checked by several host threads (the first error in
+// batch order is reported, as a sequential check would)
+Status validate_indexes(const hpgb_gridder* g, const void* vis, size_t n) {
+  constexpr size_t kPerThread = size_t(1) << 18;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>(std::min<size_t>(hw, 32),
+                                     (n + kPerThread - 1) / kPerThread);
+  if (nt <= 1) return validate_range(g, vis, n);
+  const size_t rec = visdata_size(g->npol);
+  const size_t per = (n + nt - 1) / nt;
+  std::vector<Status> res(nt);
+  std::vector<std::thread> th;
+  th.reserve(nt);
+  for (size_t t = 0; t < nt; ++t)
+    th.emplace_back([&, t]() {
+      const size_t a = t * per, b = std::min(n, a + per);
+      if (a < b) {
+        res[t] = validate_range(
+            g, static_cast<const char*>(vis) + a * rec, b - a);
+        if (!res[t]) {  // report the batch index, not the chunk index
+          size_t i = a;
+          while (i < b && validate_range(g, static_cast<const char*>(vis) + i * rec, 1))
+            ++i;
+          res[t] = validate_range(g, static_cast<const char*>(vis) + i * rec, 1);
+          res[t].msg = "visibility " + std::to_string(i) +
+                       res[t].msg.substr(res[t].msg.find(':'));
+        }
+      }
+    });
+  for (auto& x : th) x.join();
+  for (auto& r : res)
+    if (!r) return r;
+  return Status::ok();
 }
 
 // every Mueller index must address a Mueller plane of every CF group (the
@@ -418,14 +454,24 @@ int hpgb_grid_visibilities(hpgb_gridder* g, const void* vis, size_t n,
       return Status::err(HPGB_ERROR_OTHER, "no convolution function set");
     HPGB_TRY(validate_mueller(g));
     HPGB_CUDA_TRY(cudaSetDevice(g->device));
-    if (!vis_on_device) HPGB_TRY(validate_indexes(g, vis, n));
     const size_t rec = visdata_size(npol);
     const size_t bytes = n * rec;
     HPGB_TRY(g->vb.vis.reserve(g->max_batch * rec));
+    // the copy is queued first, so that checking the indexes of host
+    // records overlaps the transfer; a batch that fails the check is
+    // copied (the call waits for that copy, the caller may free its
+    // buffer on return) but never gridded
     HPGB_CUDA_TRY(cudaMemcpyAsync(
         g->vb.vis.ptr, vis, bytes,
         vis_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
         g->stream));
+    if (!vis_on_device) {
+      Status v = validate_indexes(g, vis, n);
+      if (!v) {
+        cudaStreamSynchronize(g->stream);
+        return v;
+      }
+    }
     HPGB_TRY(grid_batch(g, g->vb.vis.ptr, n, flags));
     if (flags & HPGB_RETURN_VISIBILITIES) {
       HPGB_CUDA_TRY(cudaMemcpyAsync(

@@ -95,8 +95,12 @@ Status autotune_tiled(hpgb_gridder* g, const void* vis, size_t n,
                      "the tiled kernel cannot take this CF or grid");
   for (int ring = 4; st && ring <= 8; ++ring) st = trial(Trial{ring, 0});
   if (st && best_ms < std::numeric_limits<float>::max()) {
-    const int base = g->precision == HPGB_PRECISION_MIXED ? 256 : 2048;
-    for (int chunk : {base / 2, base * 2, base * 4})
+    // the mixed form's FP32 tile holds at most 512 visibilities between
+    // flushes: its rounding error grows with the number summed
+    const bool mixed = g->precision == HPGB_PRECISION_MIXED;
+    const std::vector<int> chunks =
+        mixed ? std::vector<int>{128, 512} : std::vector<int>{1024, 4096, 8192};
+    for (int chunk : chunks)
       if (st) st = trial(Trial{best.ring_parts, chunk});
   }
   cudaEventDestroy(e0);
