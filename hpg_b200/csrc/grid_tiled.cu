@@ -497,7 +497,7 @@ __device__ __forceinline__ void degrid_cells(
 }
 
 // Gridding of one visibility's footprint cells c = first, first + stride,
-// ... into the row's shared-memory grid tile (src/hpg_core.hpp:856-873).
+// ... < end into the row's shared-memory grid tile (src/hpg_core.hpp:856-873).
 // The gridding warps cover every cell of one visibility between two
 // barriers, so no two threads add to a tile cell at once (measured faster
 // than shared-memory atomics with two visibilities in flight).  pp[v]: slot
@@ -509,9 +509,9 @@ template <int N, bool MIXED, bool DENSE, bool SCREEN>
 __device__ __forceinline__ void grid_cells(const VisGeom& g, const int (&pp)[N],
                                            uint32_t cfs, const float2 (&gv)[N],
                                            uint32_t gtile, int R, int first,
-                                           int stride) {
+                                           int stride, int end) {
   using GT = typename Form<MIXED>::grid_t;
-  const int tx = g.tx, ncell = g.tx * g.ty;
+  const int tx = g.tx, ncell = end;
   CellWalk w(first, stride, tx, g.inv_tx,
              gtile + uint32_t(g.cy * R + g.cx) * uint32_t(sizeof(GT)), R,
              uint32_t(sizeof(GT)));
@@ -1010,11 +1010,13 @@ tiled_kernel(const __grid_constant__ TiledParams p,
               if (vg.screen_on)
                 grid_cells<N, MIXED, DENSE, true>(
                     vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]), gv,
-                    ptx::smem(gtile), R, gw * 32 + lane, kGR * 32);
+                    ptx::smem(gtile), R, gw * 32 + lane, kGR * 32,
+                    vg.tx * vg.ty);
               else
                 grid_cells<N, MIXED, DENSE, false>(
                     vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]), gv,
-                    ptx::smem(gtile), R, gw * 32 + lane, kGR * 32);
+                    ptx::smem(gtile), R, gw * 32 + lane, kGR * 32,
+                    vg.tx * vg.ty);
             }
             TT_END(7);
           }
