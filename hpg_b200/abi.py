@@ -137,6 +137,10 @@ SIGNATURES = {
     "hpgb_set_tiled_plan": ([_P, _I, _I], _I),
     "hpgb_autotune_tiled": ([_P, _P, _S, _U, _U, _I, ctypes.POINTER(_I),
                              ctypes.POINTER(_I)], _I),
+    "hpgb_begin_capture": ([_P], _I),
+    "hpgb_end_capture": ([_P, _PP], _I),
+    "hpgb_graph_launch": ([_P, _P], _I),
+    "hpgb_graph_destroy": ([_P], _I),
     "hpgb_profile_tiled_kernel": ([_P, _I], _I),
     "hpgb_tiled_kernel_time": ([_P, ctypes.POINTER(_D),
                                 ctypes.POINTER(ctypes.c_uint64)], _I),

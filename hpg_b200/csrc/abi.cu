@@ -753,6 +753,63 @@ int hpgb_autotune_tiled(hpgb_gridder* g, const void* vis, size_t n,
   });
 }
 
+int hpgb_begin_capture(hpgb_gridder* g) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    HPGB_TRY(fence_impl(g));
+    HPGB_CUDA_TRY(
+        cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeRelaxed));
+    g->capture_launches0 = g->launches;
+    return Status::ok();
+  });
+}
+
+int hpgb_end_capture(hpgb_gridder* g, hpgb_graph** out) {
+  return guarded([&]() -> Status {
+    if (!g || !out) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    *out = nullptr;
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    cudaGraph_t graph = nullptr;
+    HPGB_CUDA_TRY(cudaStreamEndCapture(g->stream, &graph));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t rc = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (rc != cudaSuccess)
+      return Status::err(HPGB_ERROR_OTHER,
+                         std::string("cudaGraphInstantiate: ") +
+                             cudaGetErrorString(rc));
+    auto* h = new hpgb_graph;
+    h->exec = exec;
+    h->device = g->device;
+    h->launches = g->launches - g->capture_launches0;
+    *out = h;
+    return Status::ok();
+  });
+}
+
+int hpgb_graph_launch(hpgb_gridder* g, const hpgb_graph* graph) {
+  return guarded([&]() -> Status {
+    if (!g || !graph) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    if (graph->device != g->device)
+      return Status::err(HPGB_ERROR_OTHER, "graph captured on another device");
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    HPGB_CUDA_TRY(cudaGraphLaunch(graph->exec, g->stream));
+    g->launches += graph->launches;
+    return Status::ok();
+  });
+}
+
+int hpgb_graph_destroy(hpgb_graph* graph) {
+  return guarded([&]() -> Status {
+    if (!graph) return Status::ok();
+    cudaSetDevice(graph->device);
+    cudaGraphExecDestroy(graph->exec);
+    delete graph;
+    return Status::ok();
+  });
+}
+
 int hpgb_profile_tiled_kernel(hpgb_gridder* g, int enable) {
   return guarded([&]() -> Status {
     if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");

@@ -52,6 +52,13 @@ struct hpgb_gridder_impl;
 
 }  // namespace hpgb
 
+// an instantiated CUDA graph of work captured on a gridder's stream
+struct hpgb_graph {
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+  uint64_t launches = 0;  // kernels in the graph
+};
+
 struct hpgb_gridder {
   int device = 0;
   unsigned max_added_tasks = 0;
@@ -88,6 +95,7 @@ struct hpgb_gridder {
 
   mutable std::mutex mtx;
   uint64_t launches = 0;  // kernels launched by this gridder
+  uint64_t capture_launches0 = 0;  // launches when the stream capture began
 
   // event pairs around each launch of the tiled gridding kernel, recorded
   // while profiling is on (benchmark instrumentation)

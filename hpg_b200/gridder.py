@@ -359,6 +359,11 @@ class Gridder:
                                          ctypes.byref(chunk)))
         return ring.value, chunk.value
 
+    def capture(self):
+        """Context manager recording the calls inside it into a CUDA graph
+        (see hpgb_begin_capture); yields a Graph filled in at exit."""
+        return _Capture(self)
+
     def profile_tiled_kernel(self, enable=True):
         """Record CUDA events around every tiled-kernel launch (benchmark
         instrumentation)."""
@@ -385,3 +390,44 @@ class Gridder:
         check(load().hpgb_debug_coords(self._h, ptr(vis), len(vis), self.npol,
                                        ptr(out)))
         return out
+
+
+class Graph:
+    """An instantiated CUDA graph of a gridder's captured calls."""
+
+    def __init__(self, gridder):
+        self._g = gridder
+        self._h = None
+
+    def launch(self):
+        check(load().hpgb_graph_launch(self._g._h, self._h))
+
+    def close(self):
+        if self._h:
+            check(load().hpgb_graph_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Capture:
+    def __init__(self, gridder):
+        self.graph = Graph(gridder)
+
+    def __enter__(self):
+        check(load().hpgb_begin_capture(self.graph._g._h))
+        return self.graph
+
+    def __exit__(self, exc_type, exc, tb):
+        h = ctypes.c_void_p()
+        rc = load().hpgb_end_capture(self.graph._g._h, ctypes.byref(h))
+        if exc_type is None:
+            check(rc)
+            self.graph._h = h
+        elif rc == 0 and h:
+            load().hpgb_graph_destroy(h)
+        return False

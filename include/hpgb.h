@@ -359,6 +359,24 @@ HPGB_API int hpgb_autotune_tiled(hpgb_gridder* gridder, const void* visibilities
                                  int vis_on_device, int* ring_parts,
                                  int* chunk_vis);
 
+/* CUDA-graph capture of a gridder's work, no counterpart in the reference
+ * (the reference launches every kernel of a batch from the host each time).
+ * hpgb_begin_capture fences the gridder and starts capturing its stream;
+ * the calls that follow are recorded instead of run, up to
+ * hpgb_end_capture, which returns an instantiated graph; hpgb_graph_launch
+ * replays it on the gridder's stream (asynchronously, like the calls it
+ * holds).  Capture only calls whose inputs stay where they are between
+ * replays: device-resident visibilities (vis_on_device 1) or pinned host
+ * buffers, the same batch size as an uncaptured call made before the
+ * capture (so that no buffer grows), and no call that waits for the device
+ * (hpgb_fence, copies of the grid, weights or model to the host).  A graph
+ * must not outlive its gridder; destroy it with hpgb_graph_destroy. */
+typedef struct hpgb_graph hpgb_graph;
+HPGB_API int hpgb_begin_capture(hpgb_gridder* gridder);
+HPGB_API int hpgb_end_capture(hpgb_gridder* gridder, hpgb_graph** graph);
+HPGB_API int hpgb_graph_launch(hpgb_gridder* gridder, const hpgb_graph* graph);
+HPGB_API int hpgb_graph_destroy(hpgb_graph* graph);
+
 /* Benchmark instrumentation, no counterpart in the reference: while
  * enabled, CUDA events are recorded on the gridder's stream around every
  * launch of the tiled gridding kernel.  hpgb_tiled_kernel_time waits for the

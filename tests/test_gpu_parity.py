@@ -248,6 +248,36 @@ def test_autotune_keeps_data_and_parity(gpu, oracle_lib, precision):
     np.testing.assert_allclose(g.grid_weights(), o.weights, rtol=1e-12)
 
 
+@pytest.mark.parametrize("kernel,precision", KERNELS, ids=KERNEL_IDS)
+def test_graph_capture_replay(gpu, oracle_lib, kernel, precision):
+    """A degrid+grid call captured into a CUDA graph and replayed three
+    times does what three calls do."""
+    import torch
+    cfg = small_full_pol(2000, grad=0.3, seed=13)
+    dv = torch.from_numpy(cfg["vis"].view(np.uint8)).cuda()
+    ref, _ = make_pair(cfg, oracle_lib, precision=precision, kernel=kernel)
+    for _ in range(3):
+        ref.degrid_grid_visibilities(dv, on_device=True)
+    ref.fence()
+    g, _ = make_pair(cfg, oracle_lib, precision=precision, kernel=kernel)
+    g.degrid_grid_visibilities(dv, on_device=True)   # buffers reach size
+    g.fence()
+    g.reset_grid()
+    with g.capture() as graph:
+        g.degrid_grid_visibilities(dv, on_device=True)
+    before = g.kernel_launches()
+    for _ in range(3):
+        graph.launch()
+    g.fence()
+    assert g.kernel_launches() > before
+    tol = 1e-12 if precision == abi.PRECISION_FP64 else 1e-6
+    assert rel_norm(g.grid_values(), ref.grid_values()) <= tol
+    np.testing.assert_allclose(g.grid_weights(), ref.grid_weights(), rtol=1e-12)
+    graph.close()
+    g.close()
+    ref.close()
+
+
 def test_tiled_plan_rejects_shallow_ring(gpu, oracle_lib):
     """A ring of fewer than four parts could stall the pipeline: refused."""
     cfg = small_full_pol(10)
