@@ -131,6 +131,7 @@ SIGNATURES = {
     "hpgb_normalize_by_weights": ([_P, _D], _I),
     "hpgb_apply_grid_fft": ([_P, _D, _I, _I], _I),
     "hpgb_apply_model_fft": ([_P, _D, _I, _I], _I),
+    "hpgb_image_grid": ([_P, _D, _D, _I, _I], _I),
     "hpgb_shift_grid": ([_P, _I], _I),
     "hpgb_shift_model": ([_P, _I], _I),
     "hpgb_kernel_launches": ([_P, ctypes.POINTER(ctypes.c_uint64)], _I),

@@ -686,6 +686,15 @@ int hpgb_apply_model_fft(hpgb_gridder* g, double norm, int sign, int in_place) {
   });
 }
 
+int hpgb_image_grid(hpgb_gridder* g, double wfactor, double norm, int sign,
+                    int direction) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    HPGB_CUDA_TRY(cudaSetDevice(g->device));
+    return image_tail(g, wfactor, norm, sign, direction);
+  });
+}
+
 int hpgb_shift_grid(hpgb_gridder* g, int direction) {
   return guarded([&]() -> Status {
     if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");

@@ -156,5 +156,7 @@ Status to_layout(hpgb_gridder* g, const double2* src, double2* dst,
 Status weights_to_layout(hpgb_gridder* g, const double* src, double* dst,
                          int layout);
 void release_fft_plans(hpgb_gridder* g);
+Status image_tail(hpgb_gridder* g, double wfactor, double norm, int sign,
+                  int direction);
 
 }  // namespace hpgb

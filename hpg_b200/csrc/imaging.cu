@@ -72,6 +72,62 @@ __global__ void shift_even_kernel(double2* __restrict__ grid, int nx, int ny,
   }
 }
 
+// per-plane factor of the imaging tail: 1 / (wfactor * weight) then 1 / norm
+__device__ __forceinline__ double2 tail_scale(double2 v, const double* weights,
+                                              size_t p, double wfactor,
+                                              double inv_norm) {
+  const double d = __dmul_rn(wfactor, weights[p]);
+  v.x = __dmul_rn(__ddiv_rn(v.x, d), inv_norm);
+  v.y = __dmul_rn(__ddiv_rn(v.y, d), inv_norm);
+  return v;
+}
+
+// shift_even_kernel with the imaging tail's per-plane scaling folded in
+__global__ void shift_even_scale_kernel(double2* __restrict__ grid, int nx,
+                                        int ny, size_t nplanes,
+                                        const double* __restrict__ weights,
+                                        double wfactor, double inv_norm) {
+  const int mx = nx / 2, my = ny / 2;
+  const size_t quarter = size_t(mx) * my;
+  const size_t plane = size_t(nx) * ny;
+  const size_t n = quarter * nplanes;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const size_t p = i / quarter;
+    const size_t r = i - p * quarter;
+    const int y = int(r / mx), x = int(r - size_t(y) * mx);
+    double2* pl = grid + p * plane;
+    const size_t a = size_t(y) * nx + x, b = size_t(y + my) * nx + (x + mx);
+    const size_t c = size_t(y) * nx + (x + mx), d = size_t(y + my) * nx + x;
+    const double2 va = pl[a], vb = pl[b], vc = pl[c], vd = pl[d];
+    pl[a] = tail_scale(vb, weights, p, wfactor, inv_norm);
+    pl[b] = tail_scale(va, weights, p, wfactor, inv_norm);
+    pl[c] = tail_scale(vd, weights, p, wfactor, inv_norm);
+    pl[d] = tail_scale(vc, weights, p, wfactor, inv_norm);
+  }
+}
+
+// roll_kernel with the imaging tail's per-plane scaling folded in
+__global__ void roll_scale_kernel(const double2* __restrict__ in,
+                                  double2* __restrict__ out, int nx, int ny,
+                                  int sx, int sy, size_t nplanes,
+                                  const double* __restrict__ weights,
+                                  double wfactor, double inv_norm) {
+  const size_t plane = size_t(nx) * ny;
+  const size_t n = plane * nplanes;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const size_t p = i / plane;
+    const size_t r = i - p * plane;
+    const int y = int(r / nx), x = int(r - size_t(y) * nx);
+    int xs = x - sx, ys = y - sy;
+    xs = ((xs % nx) + nx) % nx;
+    ys = ((ys % ny) + ny) % ny;
+    out[i] = tail_scale(in[p * plane + size_t(ys) * nx + xs], weights, p,
+                        wfactor, inv_norm);
+  }
+}
+
 // general sizes: out(x, y) = in(x - sx mod nx, y - sy mod ny)
 __global__ void roll_kernel(const double2* __restrict__ in,
                             double2* __restrict__ out, int nx, int ny, int sx,
@@ -152,6 +208,44 @@ Status shift(hpgb_gridder* g, double2* grid, int direction) {
   HPGB_TRY(tmp.reserve(n * sizeof(double2)));
   roll_kernel<<<blocks_for(n, 256), 256, 0, g->stream>>>(
       grid, tmp.as<double2>(), nx, ny, sx, sy, np);
+  HPGB_CUDA_TRY(cudaGetLastError());
+  ++g->launches;
+  HPGB_CUDA_TRY(cudaMemcpyAsync(grid, tmp.ptr, n * sizeof(double2),
+                                cudaMemcpyDeviceToDevice, g->stream));
+  HPGB_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  return Status::ok();
+}
+
+// The imaging tail normalize_by_weights(wfactor) -> apply_grid_fft(norm,
+// sign, in place) -> shift_grid(direction) (src/hpg_runtime.hpp:1293-1441)
+// as the FFT followed by one pass: the normalisation is a factor per
+// (mrow, cube) plane and the FFT transforms each plane linearly, so the
+// factor is applied after the FFT, together with 1/norm, in the pass that
+// shifts (results equal the three calls' to FP64 rounding).
+Status image_tail(hpgb_gridder* g, double wfactor, double norm, int sign,
+                  int direction) {
+  HPGB_TRY(fft(g, g->grid, 1.0, sign, true));
+  const int nx = int(g->grid_size[0]), ny = int(g->grid_size[1]);
+  const size_t np = size_t(g->grid_size[2]) * g->grid_size[3];
+  const double inv_norm = 1.0 / norm;
+  double2* grid = g->grid.as<double2>();
+  const double* w = g->weights.as<const double>();
+  if (nx % 2 == 0 && ny % 2 == 0) {
+    const size_t n = size_t(nx / 2) * (ny / 2) * np;
+    if (n == 0) return Status::ok();
+    shift_even_scale_kernel<<<blocks_for(n, 256), 256, 0, g->stream>>>(
+        grid, nx, ny, np, w, wfactor, inv_norm);
+    HPGB_CUDA_TRY(cudaGetLastError());
+    ++g->launches;
+    return Status::ok();
+  }
+  const int sx = direction == HPGB_SHIFT_FORWARD ? nx / 2 : -(nx / 2);
+  const int sy = direction == HPGB_SHIFT_FORWARD ? ny / 2 : -(ny / 2);
+  const size_t n = g->grid_elems();
+  DevBuf tmp;
+  HPGB_TRY(tmp.reserve(n * sizeof(double2)));
+  roll_scale_kernel<<<blocks_for(n, 256), 256, 0, g->stream>>>(
+      grid, tmp.as<double2>(), nx, ny, sx, sy, np, w, wfactor, inv_norm);
   HPGB_CUDA_TRY(cudaGetLastError());
   ++g->launches;
   HPGB_CUDA_TRY(cudaMemcpyAsync(grid, tmp.ptr, n * sizeof(double2),

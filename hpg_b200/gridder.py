@@ -309,6 +309,14 @@ class Gridder:
     def model_values_ptr(self):
         return self._device_ptr(load().hpgb_model_device_ptr)
 
+    def image_grid(self, wfactor=1.0, norm=1.0, sign=None, direction=None):
+        """normalize_by_weights(wfactor), apply_grid_fft(norm, sign) and
+        shift_grid(direction) as one FFT and one pass over the grid."""
+        sign = abi.FFT_POSITIVE if sign is None else int(sign)
+        direction = abi.SHIFT_FORWARD if direction is None else int(direction)
+        check(load().hpgb_image_grid(self._h, float(wfactor), float(norm),
+                                     sign, direction))
+
     def reset_grid(self):
         check(load().hpgb_reset_grid(self._h))
 

@@ -327,6 +327,15 @@ HPGB_API int hpgb_apply_grid_fft(hpgb_gridder* gridder, double norm, int sign,
 HPGB_API int hpgb_apply_model_fft(hpgb_gridder* gridder, double norm, int sign,
                          int in_place);
 
+/* The imaging tail in one call: the effect of hpgb_normalize_by_weights
+ * (wfactor), hpgb_apply_grid_fft(norm, sign, in place) and
+ * hpgb_shift_grid(direction) in that order, done as the FFT and one pass
+ * over the grid (the per-plane normalisation commutes with the FFT and is
+ * applied with 1/norm in the shift's pass); equal to the three calls to
+ * FP64 rounding.  No counterpart in the reference. */
+HPGB_API int hpgb_image_grid(hpgb_gridder* gridder, double wfactor, double norm,
+                             int sign, int direction);
+
 /* State::shift_grid / shift_model (:198-202, impl :1428-1456). */
 HPGB_API int hpgb_shift_grid(hpgb_gridder* gridder, int direction);
 HPGB_API int hpgb_shift_model(hpgb_gridder* gridder, int direction);

@@ -380,6 +380,29 @@ def test_normalize_fft_shift(gpu, oracle_lib):
     assert rel_norm(g.grid_values(), ref2) <= 1e-12
 
 
+@pytest.mark.parametrize("side", [256, 255])
+@pytest.mark.parametrize("sign,direction", [(abi.FFT_POSITIVE, abi.SHIFT_FORWARD),
+                                            (abi.FFT_NEGATIVE, abi.SHIFT_BACKWARD)])
+def test_image_grid_equals_three_calls(gpu, oracle_lib, side, sign, direction):
+    """The fused imaging tail against normalize_by_weights, apply_grid_fft
+    and shift_grid called in turn."""
+    cfg = workloads.full_pol_config(3000, grid=side, oversampling=16,
+                                    supports=(4, 6, 8), seed=17)
+    g, _ = make_pair(cfg, oracle_lib, kernel="tiled")
+    g.grid_visibilities(cfg["vis"])
+    g.fence()
+    h = g.copy()
+    g.normalize_by_weights(0.5)
+    g.apply_grid_fft(3.0, sign)
+    g.shift_grid(direction)
+    h.image_grid(0.5, 3.0, sign, direction)
+    a, b = g.grid_values(), h.grid_values()
+    assert np.abs(a).max() > 0
+    assert rel_norm(b, a) <= 1e-12
+    g.close()
+    h.close()
+
+
 @pytest.mark.parametrize("size", [(20, 20), (19, 19), (18, 19), (19, 18)])
 def test_shift_cycle(gpu, oracle_lib, size):
     """GridderState.ShiftCycle (:1860-1926)."""
