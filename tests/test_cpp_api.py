@@ -34,3 +34,16 @@ def test_cpp_api_on_device(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.strip().endswith("OK")
+
+
+def test_cpp_indexer(tmp_path):
+    """hpgb::CFSimpleIndexer (header only) against the reference's cases."""
+    exe = str(tmp_path / "test_indexing")
+    subprocess.run(
+        ["g++", "-std=c++17", "-O1", "-Wall",
+         "-I" + os.path.join(ROOT, "hpg_b200", "cpp", "include"),
+         os.path.join(ROOT, "tests", "cpp", "test_indexing.cc"), "-o", exe],
+        check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip() == "OK"
