@@ -505,21 +505,45 @@ __device__ __forceinline__ void degrid_cells(
 // gv[v] arrive conjugated when w > 0 (the CF imaginary part is negated
 // then): conj(cf)*s*g = conj(cf*conj(s)*conj(g)), bit for bit in the
 // reference's FP32 products, so only the sum's imaginary part flips.
+// Loop state of grid_cells, formed from the descriptor alone: the gridding
+// warps set it up while they still wait for the visibility's gridding
+// values, so its address arithmetic is off the critical path.
+template <int N>
+struct GridCursor {
+  CellWalk w;
+  uint32_t po[N];  // plane offsets in bytes
+  uint32_t ca, dca;
+  int first, stride, end;
+};
+
+template <int N, bool MIXED>
+__device__ __forceinline__ GridCursor<N> grid_prepare(
+    const VisGeom& g, const int (&pp)[N], uint32_t cfs, uint32_t gtile, int R,
+    int first, int stride, int end) {
+  using GT = typename Form<MIXED>::grid_t;
+  GridCursor<N> k{CellWalk(first, stride, g.tx, g.inv_tx,
+                           gtile + uint32_t(g.cy * R + g.cx) * uint32_t(sizeof(GT)),
+                           R, uint32_t(sizeof(GT)))};
+#pragma unroll
+  for (int v = 0; v < N; ++v)
+    k.po[v] = uint32_t((pp[v] >= 0 ? pp[v] : 0) * g.pst) * 8u;
+  k.ca = cfs + uint32_t(first) * 8u;
+  k.dca = uint32_t(stride) * 8u;
+  k.first = first;
+  k.stride = stride;
+  k.end = end;
+  return k;
+}
+
 template <int N, bool MIXED, bool DENSE, bool SCREEN>
 __device__ __forceinline__ void grid_cells(const VisGeom& g, const int (&pp)[N],
-                                           uint32_t cfs, const float2 (&gv)[N],
-                                           uint32_t gtile, int R, int first,
-                                           int stride, int end) {
-  using GT = typename Form<MIXED>::grid_t;
-  const int tx = g.tx, ncell = end;
-  CellWalk w(first, stride, tx, g.inv_tx,
-             gtile + uint32_t(g.cy * R + g.cx) * uint32_t(sizeof(GT)), R,
-             uint32_t(sizeof(GT)));
-  uint32_t po[N];
-#pragma unroll
-  for (int v = 0; v < N; ++v) po[v] = uint32_t((pp[v] >= 0 ? pp[v] : 0) * g.pst) * 8u;
-  uint32_t ca = cfs + uint32_t(first) * 8u;
-  const uint32_t dca = uint32_t(stride) * 8u;
+                                           GridCursor<N> k,
+                                           const float2 (&gv)[N]) {
+  const int tx = g.tx, ncell = k.end, first = k.first, stride = k.stride;
+  CellWalk& w = k.w;
+  const uint32_t(&po)[N] = k.po;
+  uint32_t ca = k.ca;
+  const uint32_t dca = k.dca;
   for (int c = first; c < ncell; c += stride) {
     float2 screen = make_float2(1.0f, 0.0f);
     if constexpr (SCREEN) {
@@ -992,31 +1016,32 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           TT_END(1);
           if (p.do_grid) {
             const int gs = int(q % uint32_t(kSlots));
+            // the loop state needs only the descriptor: formed before the
+            // wait for the gridding values
+            const VisGeom vg = vis_geom(descs[s]);
+            int pp[N];
+#pragma unroll
+            for (int v = 0; v < N; ++v)
+              pp[v] = int(int8_t((vg.pos_w ? gpk[1] : gpk[0]) >> (8 * v)));
+            const GridCursor<N> cur = grid_prepare<N, MIXED>(
+                vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]),
+                ptx::smem(gtile), R, gw * 32 + lane, kGR * 32, vg.tx * vg.ty);
             TT_BEGIN();
             ok &= ptx::mbar_wait(&gvfull[gs], (q / kSlots) & 1, abort);
             if (k > 0) ptx::named_sync(2, kGR * 32);
             TT_END(6);
             TT_BEGIN();
             if (!ptx::warp_flag(abort)) {
-              const VisGeom vg = vis_geom(descs[s]);
-              int pp[N];
               float2 gv[N];
 #pragma unroll
               for (int v = 0; v < N; ++v) {
-                pp[v] = int(int8_t((vg.pos_w ? gpk[1] : gpk[0]) >> (8 * v)));
                 gv[v] = gvring[gs * 4 + v];
                 if (vg.pos_w) gv[v].y = -gv[v].y;
               }
               if (vg.screen_on)
-                grid_cells<N, MIXED, DENSE, true>(
-                    vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]), gv,
-                    ptx::smem(gtile), R, gw * 32 + lane, kGR * 32,
-                    vg.tx * vg.ty);
+                grid_cells<N, MIXED, DENSE, true>(vg, pp, cur, gv);
               else
-                grid_cells<N, MIXED, DENSE, false>(
-                    vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]), gv,
-                    ptx::smem(gtile), R, gw * 32 + lane, kGR * 32,
-                    vg.tx * vg.ty);
+                grid_cells<N, MIXED, DENSE, false>(vg, pp, cur, gv);
             }
             TT_END(7);
           }
