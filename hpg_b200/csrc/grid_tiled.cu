@@ -48,8 +48,9 @@
 //         (FMA), gridding products in FP32 with the reference's rounding
 //         (cf*screen*gvis, no contraction), FP64 sum over polarizations, FP64
 //         shared-memory tile.
-//   MIXED FP32 model tile, FP32 products and per-thread FP32 partial sums
-//         (merged in FP64 across threads, rows and in the normalisation),
+//   MIXED FP32 model tile, FP32 products, per-thread and per-warp FP32
+//         partial sums (merged in FP64 across warps, rows and in the
+//         normalisation),
 //         FP32 shared-memory tile flushed into the FP64 grid every chunk.
 //         Coordinates, phases, normalisers and weight sums stay FP64.
 
@@ -839,17 +840,20 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           }
           // warp sum of the 8 (padded) partials: halve the values held per
           // lane at each of the first three levels, then butterfly; lane
-          // L ends with the sum of value ((L>>4)&1)*4 + ((L>>3)&1)*2 + ((L>>2)&1)
-          double v8[8];
+          // L ends with the sum of value ((L>>4)&1)*4 + ((L>>3)&1)*2 + ((L>>2)&1).
+          // The mixed form's partials are FP32 (exact in acc) and are summed
+          // across the warp in FP32, the FP64 form's in FP64.
+          using RR = typename std::conditional<MIXED, float, double>::type;
+          RR v8[8];
 #pragma unroll
-          for (int t = 0; t < 8; ++t) v8[t] = t < 2 * N ? acc[t] : 0.0;
-          double v4[4], v2[2], v1;
+          for (int t = 0; t < 8; ++t) v8[t] = t < 2 * N ? RR(acc[t]) : RR(0);
+          RR v4[4], v2[2], v1;
           {
             const bool hi = lane & 16;
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-              const double give = hi ? v8[i] : v8[i + 4];
-              const double keep = hi ? v8[i + 4] : v8[i];
+              const RR give = hi ? v8[i] : v8[i + 4];
+              const RR keep = hi ? v8[i + 4] : v8[i];
               v4[i] = keep + __shfl_xor_sync(0xffffffffu, give, 16);
             }
           }
@@ -857,15 +861,15 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             const bool hi = lane & 8;
 #pragma unroll
             for (int i = 0; i < 2; ++i) {
-              const double give = hi ? v4[i] : v4[i + 2];
-              const double keep = hi ? v4[i + 2] : v4[i];
+              const RR give = hi ? v4[i] : v4[i + 2];
+              const RR keep = hi ? v4[i + 2] : v4[i];
               v2[i] = keep + __shfl_xor_sync(0xffffffffu, give, 8);
             }
           }
           {
             const bool hi = lane & 4;
-            const double give = hi ? v2[0] : v2[1];
-            const double keep = hi ? v2[1] : v2[0];
+            const RR give = hi ? v2[0] : v2[1];
+            const RR keep = hi ? v2[1] : v2[0];
             v1 = keep + __shfl_xor_sync(0xffffffffu, give, 4);
           }
           v1 += __shfl_xor_sync(0xffffffffu, v1, 2);
@@ -876,7 +880,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           const int b = int(q & 1);
           if (q >= 2) ok &= ptx::mbar_wait(&dgempty[b], ((q >> 1) & 1) ^ 1, abort);
           if (ptx::warp_flag(abort)) continue;
-          if ((lane & 3) == 0) dgpart[(b * kDG + warp) * 8 + vidx] = v1;
+          if ((lane & 3) == 0) dgpart[(b * kDG + warp) * 8 + vidx] = double(v1);
           __syncwarp();
           if (lane == 0) {
             ptx::mbar_arrive(&dgfull[b]);
