@@ -892,17 +892,19 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         // -------- exchange warps --------
         // Exchange warp xw takes the visibilities q with q % 2 == xw (the
         // degrid partial buffer q % 2 is its own).  For each of them it
-        // sends this row's partials to every CTA of the cluster, then
-        // finishes its previous visibility, whose partials from the other
-        // rows were sent one step earlier and have normally arrived.
+        // sends this row's partials to every CTA of the cluster, waits for
+        // the other rows' partials and finishes the visibility at once, so
+        // that its ring part is released as early as possible (the other
+        // exchange warp meanwhile takes the next visibility).  A remote CTA
+        // sends into exchange buffer q % 8 again only for q + 8, after it
+        // finished q + 6, which needed this CTA's partials of q + 6, sent
+        // after this warp finished q: the buffer is never overwritten while
+        // it is read.
         const int xw = warp - kXBase;
-        int prev_s = -1;
-        uint32_t prev_q = 0;
-        for (int k = 0; k <= ch.count; ++k) {
-          const bool mine = k < ch.count && (q & 1) == uint32_t(xw);
-          int s = -1;
-          if (mine) {
-            s = int(q % uint32_t(kSlots));
+        for (int k = 0; k < ch.count; ++k, ++q) {
+          if ((q & 1) != uint32_t(xw)) continue;
+          {
+            const int s = int(q % uint32_t(kSlots));
             TT_BEGIN();
             ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
             TT_END(1);
@@ -933,10 +935,11 @@ tiled_kernel(const __grid_constant__ TiledParams p,
               TT_END(4);
             }
           }
-          if ((mine || k == ch.count) && prev_s >= 0) {
+          {
+            const int s = int(q % uint32_t(kSlots));
             TT_BEGIN();
-            const uint32_t qq = prev_q;
-            const TileDesc& d = descs[prev_s];
+            const uint32_t qq = q;
+            const TileDesc& d = descs[s];
             const int xs = int(qq % uint32_t(kXSlots));
             const int gs = int(qq % uint32_t(kSlots));
             // everything the finish needs from the descriptor is read
@@ -995,17 +998,11 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             __syncwarp();
             if (live && lane == 0) {
               if (p.do_grid) ptx::mbar_arrive(&gvfull[gs]);
-              ptx::mbar_arrive(&empty[prev_s]);
+              ptx::mbar_arrive(&empty[s]);
             }
             __syncwarp();
-            prev_s = -1;
             TT_END(5);
           }
-          if (mine) {
-            prev_s = s;
-            prev_q = q;
-          }
-          if (k < ch.count) ++q;
         }
       } else {
         // -------- gridding warps --------
