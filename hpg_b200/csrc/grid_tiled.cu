@@ -464,10 +464,17 @@ __device__ __forceinline__ void degrid_cells(
 #pragma unroll
     for (int v = 0; v < N; ++v) acc[2 * v + 1] *= sgn;
   } else {
+    // Packed FP32 products (two per instruction): per plane v the thread
+    // sums P = sum cf * (mx, mx) and Q = sum cf * (my, my) componentwise;
+    // then Re = P.x - sgn Q.y and Im = Q.x + sgn P.y are the real and
+    // imaginary parts of sum cf' * m (the imaginary part already times sgn).
     const float sgn = g.pos_w ? 1.0f : -1.0f;
-    float a[2 * N];
+    float2 P[N], Q[N];
 #pragma unroll
-    for (int k = 0; k < 2 * N; ++k) a[k] = 0.f;
+    for (int v = 0; v < N; ++v) {
+      P[v] = make_float2(0.f, 0.f);
+      Q[v] = make_float2(0.f, 0.f);
+    }
     for (int c = first; c < ncell; c += stride) {
       float2 mv = ptx::lds_f2(w.tile);
       if constexpr (SCREEN) {
@@ -477,13 +484,13 @@ __device__ __forceinline__ void degrid_cells(
         const float sx = float(sc.x), sy = float(sc.y);
         mv = make_float2(mv.x * sx - mv.y * sy, mv.x * sy + mv.y * sx);
       }
-      const float my = sgn * mv.y;
+      const float2 xx = make_float2(mv.x, mv.x), yy = make_float2(mv.y, mv.y);
 #pragma unroll
       for (int v = 0; v < N; ++v) {
         if (DENSE || pp[v] >= 0) {
           const float2 cf = ptx::lds_f2(ca + po[v]);
-          a[2 * v] = fmaf(cf.x, mv.x, fmaf(-cf.y, my, a[2 * v]));
-          a[2 * v + 1] = fmaf(cf.x, my, fmaf(cf.y, mv.x, a[2 * v + 1]));
+          P[v] = __ffma2_rn(cf, xx, P[v]);
+          Q[v] = __ffma2_rn(cf, yy, Q[v]);
         }
       }
       w.next(tx);
@@ -491,8 +498,8 @@ __device__ __forceinline__ void degrid_cells(
     }
 #pragma unroll
     for (int v = 0; v < N; ++v) {
-      acc[2 * v] = a[2 * v];
-      acc[2 * v + 1] = double(a[2 * v + 1]) * double(sgn);
+      acc[2 * v] = fmaf(-sgn, Q[v].y, P[v].x);
+      acc[2 * v + 1] = fmaf(sgn, P[v].y, Q[v].x);
     }
   }
 }
@@ -545,6 +552,18 @@ __device__ __forceinline__ void grid_cells(const VisGeom& g, const int (&pp)[N],
   const uint32_t(&po)[N] = k.po;
   uint32_t ca = k.ca;
   const uint32_t dca = k.dca;
+  // mixed form: with s = -1 for w > 0 (else +1) and g' = gv[v], the cell
+  // gains (sum cf.x g'.x - cf.y g'.y, s * sum cf.x g'.y + cf.y g'.x), which
+  // is (s1.x + s2.y, s1.y + s2.x) for ga = (g'.x, s g'.x), gb = (s g'.y, -g'.y)
+  float2 ga[N], gb[N];
+  if constexpr (MIXED) {
+    const float sg = g.pos_w ? -1.0f : 1.0f;
+#pragma unroll
+    for (int v = 0; v < N; ++v) {
+      ga[v] = make_float2(gv[v].x, sg * gv[v].x);
+      gb[v] = make_float2(sg * gv[v].y, -gv[v].y);
+    }
+  }
   for (int c = first; c < ncell; c += stride) {
     float2 screen = make_float2(1.0f, 0.0f);
     if constexpr (SCREEN) {
@@ -572,7 +591,9 @@ __device__ __forceinline__ void grid_cells(const VisGeom& g, const int (&pp)[N],
       t.y = g.pos_w ? t.y - sy : t.y + sy;
       ptx::sts_d2(w.tile, t);
     } else {
-      float sx = 0.f, sy = 0.f;
+      // packed FP32 products: s1 = sum cf * ga[v], s2 = sum cf * gb[v]
+      // componentwise, and the cell's increment is (s1.x + s2.y, s1.y + s2.x)
+      float2 s1 = make_float2(0.f, 0.f), s2 = make_float2(0.f, 0.f);
 #pragma unroll
       for (int v = 0; v < N; ++v) {
         if (DENSE || pp[v] >= 0) {
@@ -580,14 +601,12 @@ __device__ __forceinline__ void grid_cells(const VisGeom& g, const int (&pp)[N],
           if constexpr (SCREEN)
             cf = make_float2(cf.x * screen.x - cf.y * screen.y,
                              cf.x * screen.y + cf.y * screen.x);
-          sx = fmaf(cf.x, gv[v].x, fmaf(-cf.y, gv[v].y, sx));
-          sy = fmaf(cf.x, gv[v].y, fmaf(cf.y, gv[v].x, sy));
+          s1 = __ffma2_rn(cf, ga[v], s1);
+          s2 = __ffma2_rn(cf, gb[v], s2);
         }
       }
-      float2 t = ptx::lds_f2(w.tile);
-      t.x += sx;
-      t.y = g.pos_w ? t.y - sy : t.y + sy;
-      ptx::sts_f2(w.tile, t);
+      const float2 t = ptx::lds_f2(w.tile);
+      ptx::sts_f2(w.tile, __fadd2_rn(t, make_float2(s1.x + s2.y, s1.y + s2.x)));
     }
     w.next(tx);
     ca += dca;
