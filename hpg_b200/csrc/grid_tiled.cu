@@ -16,8 +16,8 @@
 //                         weights from the per-slice CF sums, gridding
 //                         values) + the address of its CF slice
 //   5. tiled_kernel       persistent, one thread-block cluster per tile with
-//                         one CTA per grid row (Mueller row) r; 19 warps:
-//                         - a producer warp streams each visibility's
+//                         one CTA per grid row (Mueller row) r; 20 warps:
+//                         - two producer warps stream each visibility's
 //                           descriptor and the CF planes row r needs
 //                           (Mueller row r of both index sets) into a ring of
 //                           shared-memory slots with cp.async.bulk and
@@ -90,7 +90,12 @@ constexpr int kPWarp = kGRBase + kGR;
 constexpr int kXSlots = 8;  // exchange buffers (visibility q uses q % 8)
 constexpr int kConsumers = (kDG + kX + kGR) * 32;
 static_assert(kDGGroups == kX, "degridding group g hands visibilities to exchange warp g");
-constexpr int kThreadsTiled = kConsumers + 32;
+// two producer warps: a warp's bulk copies are taken up one after another
+// (measured on B200: one warp streams ~21 B/clk per SM in ~18 KB copies, two
+// warps ~37 B/clk), so kPWarp allocates ring space for every visibility and
+// issues the copies of the even ones, kPWarp + 1 those of the odd ones
+constexpr int kProducers = 2;
+constexpr int kThreadsTiled = kConsumers + 32 * kProducers;
 constexpr int kSlots = 16;  // descriptor slots (visibilities in flight)
 constexpr int kChunkVisFP64 = 2048;
 constexpr int kChunkVisMixed = 256;
@@ -181,13 +186,15 @@ __host__ __device__ inline SmemLayout smem_layout(int ring_bytes, int R,
                                                   int esize_grid) {
   SmemLayout L;
   // mbarriers full[kSlots] empty[kSlots] model xchg[kXSlots] dgfull[2]
-  // dgempty[2] gvfull[kSlots], then the abort flag
+  // dgempty[2] gvfull[kSlots] req[kSlots], then the abort flag
   L.bars = 0;
-  L.xbuf = align_up((3 * kSlots + kXSlots + 5) * 8 + 8, 16);  // [kXSlots][4 rows][4 pol] complex double
+  L.xbuf = align_up((4 * kSlots + kXSlots + 5) * 8 + 8, 16);  // [kXSlots][4 rows][4 pol] complex double
   L.wred = L.xbuf + kXSlots * 4 * 4 * 16;  // [2][kDG][8] double (degrid partials)
   L.bcast = L.wred + 2 * kDG * 8 * 8; // [kSlots][4] float2 (gridding values)
-  L.slots = L.bcast + kSlots * 4 * 8;  // ring_off[kSlots] int, slot_end[kSlots] u64
-  L.desc = align_up(L.slots + kSlots * 4 + kSlots * 8, 128);
+  // slot_end[kSlots] u64, req_src[kSlots] i64, ring_off[kSlots] int,
+  // req_off[kSlots] int, req_pst[kSlots] int, req_desc[kSlots] int
+  L.slots = L.bcast + kSlots * 4 * 8;
+  L.desc = align_up(L.slots + kSlots * (8 + 8 + 4 + 4 + 4 + 4), 128);
   L.ring = align_up(L.desc + kSlots * int(sizeof(TileDesc)), 1024);
   L.model = align_up(L.ring + ring_bytes, 1024);
   L.grid = align_up(L.model + R * R * esize_model, 128);
@@ -633,16 +640,22 @@ tiled_kernel(const __grid_constant__ TiledParams p,
   uint64_t* dgfull = xchg + kXSlots;  // [2]
   uint64_t* dgempty = dgfull + 2;  // [2]
   uint64_t* gvfull = dgempty + 2;  // [kSlots]
-  volatile int* abort = reinterpret_cast<volatile int*>(gvfull + kSlots);
+  // copy requests of odd visibilities, from kPWarp to kPWarp + 1
+  uint64_t* req = gvfull + kSlots;  // [kSlots]
+  volatile int* abort = reinterpret_cast<volatile int*>(req + kSlots);
   double* xbuf = reinterpret_cast<double*>(sm + L.xbuf);  // [8][4][4][2]
   double* dgpart = reinterpret_cast<double*>(sm + L.wred);  // [2][kDG][8]
   // gridding values of visibility q in entry q % kSlots: the exchange warp
   // runs at most kSlots - 1 visibilities ahead of the gridding warps (the
   // producer reclaims a slot only after they are done with it)
   float2* gvring = reinterpret_cast<float2*>(sm + L.bcast);  // [kSlots][4]
-  int* ring_off = reinterpret_cast<int*>(sm + L.slots);  // [kSlots]
   unsigned long long* slot_end =
-      reinterpret_cast<unsigned long long*>(sm + L.slots + kSlots * 4);
+      reinterpret_cast<unsigned long long*>(sm + L.slots);  // [kSlots]
+  long long* req_src = reinterpret_cast<long long*>(slot_end + kSlots);
+  int* ring_off = reinterpret_cast<int*>(req_src + kSlots);  // [kSlots]
+  int* req_off = ring_off + kSlots;   // ring offset of a requested copy
+  int* req_pst = req_off + kSlots;    // its CF plane stride
+  int* req_desc = req_pst + kSlots;   // its descriptor index
   TileDesc* descs = reinterpret_cast<TileDesc*>(sm + L.desc);
   unsigned char* ring = sm + L.ring;
   MT* mtile = reinterpret_cast<MT*>(sm + L.model);
@@ -669,6 +682,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       ptx::mbar_init(&dgempty[x], 1);
     }
     for (int x = 0; x < kSlots; ++x) ptx::mbar_init(&gvfull[x], 1);
+    for (int x = 0; x < kSlots; ++x) ptx::mbar_init(&req[x], 1);
     *abort = 0;
     ptx::fence_mbar_init();
   }
@@ -690,14 +704,15 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       gpk[w] |= uint32_t(p.gpos[row][w][v] & 0xff) << (8 * v);
     }
 
-  if (warp == kPWarp) {
-    // ---------------- producer warp ----------------
-    // Lane k holds the slice reference of visibility base+k of the current
-    // chunk; per visibility the warp reserves a descriptor slot and room in
-    // the byte ring, and lane 0 issues the bulk copies of its descriptor and
-    // of the CF planes of this CTA's row.  (An L2 prefetch of later slices
-    // was measured to slow the kernel: the ring already keeps enough copies
-    // in flight to cover the HBM latency.)
+  if (warp >= kPWarp) {
+    // ---------------- producer warps ----------------
+    // kPWarp: lane k holds the slice reference of visibility base+k of the
+    // current chunk; per visibility the warp reserves a descriptor slot and
+    // room in the byte ring, and lane 0 issues the bulk copies of its
+    // descriptor and of the CF planes of this CTA's row for even
+    // visibilities, or hands the copies of odd ones to kPWarp + 1 (req).
+    // (An L2 prefetch of later slices was measured to slow the kernel: the
+    // ring already keeps enough copies in flight to cover the HBM latency.)
     // this row's plane runs, held in registers (loops below are unrolled)
     const int nruns = p.nruns[row];
     const int nplanes = p.nplanes[row];
@@ -708,83 +723,113 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       run_len[u] = p.run_len[row][u];
       run_dst[u] = p.run_dst[row][u];
     }
-    uint32_t q = 0;
-    uint32_t q_old = 0;               // oldest visibility not yet reclaimed
-    unsigned long long head = 0;      // ring bytes allocated (monotonic)
-    uint32_t pos = 0;                 // head modulo the ring size
-    unsigned long long tail = 0;      // ring bytes released (monotonic)
-    TT_DECL(2);
-    for (unsigned c = cid; c < nchunks; c += ncl) {
-      const Chunk ch = p.chunks[c];
-      SliceRef cur{};
-      for (int k = 0; k < ch.count; ++k, ++q) {
-        if ((k & 31) == 0) {
-          cur = SliceRef{};
-          if (k + lane < ch.count) cur = p.srefs[ch.start + k + lane];
-        }
-        const int kk = k & 31;
-        const long long off = __shfl_sync(0xffffffffu, cur.off, kk);
-        const int pstride = __shfl_sync(0xffffffffu, cur.pstride, kk);
-        // Reclaim the oldest visibilities' slots until a descriptor slot
-        // is free and the CF part fits in the byte ring (allocations never
-        // straddle the ring end; they are released in order).
-        const bool cf_needed = exchange || p.do_grid;
-        const uint32_t pbytes = uint32_t(pstride) * 8u;
-        const uint32_t need = cf_needed ? uint32_t(nplanes) * pbytes : 0u;
-        const uint32_t rb = uint32_t(p.ring_bytes);
-        TT_BEGIN();
-        for (;;) {
-          unsigned long long h = head;
-          uint32_t ps = pos;
-          if (need > 0 && ps + need > rb) {
-            h += rb - ps;
-            ps = 0;
-          }
-          const bool need_slot = (q - q_old) >= uint32_t(kSlots);
-          const bool need_space = need > 0 && h + need - tail > rb;
-          if (!need_slot && !need_space) {
-            head = h;
-            pos = ps;
-            break;
-          }
-          if (q_old == q) {  // cannot happen: the plan keeps need <= ring
-            ok = false;
-            break;
-          }
-          const int so = int(q_old % uint32_t(kSlots));
-          ok &= ptx::mbar_wait(&empty[so], (q_old / kSlots) & 1, abort);
-          tail = slot_end[so];
-          ++q_old;
-        }
-        TT_END(0);
-        const int s = int(q % uint32_t(kSlots));
-        // after an abort nothing is copied into slots that may still be read
-        if (lane == 0 && !*abort) {
-          TT_BEGIN();
-          const int roff = int(pos);
-          ring_off[s] = roff;
-          slot_end[s] = head + need;
-          ptx::mbar_expect_tx(&full[s], uint32_t(sizeof(TileDesc)) + need);
-          ptx::bulk_g2s(&descs[s], &p.descs[ch.start + k],
-                        uint32_t(sizeof(TileDesc)), &full[s]);
-          if (cf_needed) {
-            unsigned char* dst = ring + roff;
-            const float2* slice = p.cf + off;
+    const bool cf_needed = exchange || p.do_grid;
+    // the copies of one visibility into slot s (one thread)
+    auto issue = [&](int s, int roff, long long off, int pstride, int dindex) {
+      const uint32_t pbytes = uint32_t(pstride) * 8u;
+      const uint32_t need = cf_needed ? uint32_t(nplanes) * pbytes : 0u;
+      ring_off[s] = roff;
+      ptx::mbar_expect_tx(&full[s], uint32_t(sizeof(TileDesc)) + need);
+      ptx::bulk_g2s(&descs[s], &p.descs[dindex], uint32_t(sizeof(TileDesc)),
+                    &full[s]);
+      if (cf_needed) {
+        unsigned char* dst = ring + roff;
+        const float2* slice = p.cf + off;
 #pragma unroll
-            for (int u = 0; u < kMaxRuns; ++u)
-              if (u < nruns)
-                ptx::bulk_g2s(dst + run_dst[u] * pbytes,
-                              slice + size_t(run_plane[u]) * pstride,
-                              uint32_t(run_len[u]) * pbytes, &full[s]);
-          }
-          TT_END(1);
-        }
-        head += need;
-        pos += need;
-        __syncwarp();
+        for (int u = 0; u < kMaxRuns; ++u)
+          if (u < nruns)
+            ptx::bulk_g2s(dst + run_dst[u] * pbytes,
+                          slice + size_t(run_plane[u]) * pstride,
+                          uint32_t(run_len[u]) * pbytes, &full[s]);
       }
+    };
+    uint32_t q = 0;
+    if (warp != kPWarp) {
+      // second producer warp: the odd visibilities' copies, in order, as
+      // kPWarp requests them (it never waits for this warp)
+      for (unsigned c = cid; c < nchunks; c += ncl) {
+        const int count = p.chunks[c].count;
+        for (int k = int((q + 1) & 1); k < count; k += 2) {
+          const uint32_t qq = q + uint32_t(k);
+          const int s = int(qq % uint32_t(kSlots));
+          ok &= ptx::mbar_wait(&req[s], (qq / kSlots) & 1, abort);
+          if (lane == 0 && !*abort)
+            issue(s, req_off[s], req_src[s], req_pst[s], req_desc[s]);
+          __syncwarp();
+        }
+        q += uint32_t(count);
+      }
+    } else {
+      uint32_t q_old = 0;               // oldest visibility not yet reclaimed
+      unsigned long long head = 0;      // ring bytes allocated (monotonic)
+      uint32_t pos = 0;                 // head modulo the ring size
+      unsigned long long tail = 0;      // ring bytes released (monotonic)
+      TT_DECL(2);
+      for (unsigned c = cid; c < nchunks; c += ncl) {
+        const Chunk ch = p.chunks[c];
+        SliceRef cur{};
+        for (int k = 0; k < ch.count; ++k, ++q) {
+          if ((k & 31) == 0) {
+            cur = SliceRef{};
+            if (k + lane < ch.count) cur = p.srefs[ch.start + k + lane];
+          }
+          const int kk = k & 31;
+          const long long off = __shfl_sync(0xffffffffu, cur.off, kk);
+          const int pstride = __shfl_sync(0xffffffffu, cur.pstride, kk);
+          // Reclaim the oldest visibilities' slots until a descriptor slot
+          // is free and the CF part fits in the byte ring (allocations never
+          // straddle the ring end; they are released in order).
+          const uint32_t pbytes = uint32_t(pstride) * 8u;
+          const uint32_t need = cf_needed ? uint32_t(nplanes) * pbytes : 0u;
+          const uint32_t rb = uint32_t(p.ring_bytes);
+          TT_BEGIN();
+          for (;;) {
+            unsigned long long h = head;
+            uint32_t ps = pos;
+            if (need > 0 && ps + need > rb) {
+              h += rb - ps;
+              ps = 0;
+            }
+            const bool need_slot = (q - q_old) >= uint32_t(kSlots);
+            const bool need_space = need > 0 && h + need - tail > rb;
+            if (!need_slot && !need_space) {
+              head = h;
+              pos = ps;
+              break;
+            }
+            if (q_old == q) {  // cannot happen: the plan keeps need <= ring
+              ok = false;
+              break;
+            }
+            const int so = int(q_old % uint32_t(kSlots));
+            ok &= ptx::mbar_wait(&empty[so], (q_old / kSlots) & 1, abort);
+            tail = slot_end[so];
+            ++q_old;
+          }
+          TT_END(0);
+          const int s = int(q % uint32_t(kSlots));
+          // after an abort nothing is copied into slots that may still be read
+          if (lane == 0 && !*abort) {
+            TT_BEGIN();
+            slot_end[s] = head + need;
+            if ((q & 1) == 0) {
+              issue(s, int(pos), off, pstride, ch.start + k);
+            } else {
+              req_off[s] = int(pos);
+              req_src[s] = off;
+              req_pst[s] = pstride;
+              req_desc[s] = ch.start + k;
+              ptx::mbar_arrive(&req[s]);
+            }
+            TT_END(1);
+          }
+          head += need;
+          pos += need;
+          __syncwarp();
+        }
+      }
+      if (lane == 0) { TT_STORE(blockIdx.x * 16 + 12, 2); }
     }
-    if (lane == 0) { TT_STORE(blockIdx.x * 16 + 12, 2); }
   } else {
     // ---------------- consumer roles ----------------
     // degridding warps [0, kDG), exchange warps [kXBase, kGRBase), gridding
@@ -1305,7 +1350,7 @@ Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cfg.blockDim = dim3(kThreadsTiled);  // 18 warps
+  cfg.blockDim = dim3(kThreadsTiled);  // 20 warps
   cfg.dynamicSmemBytes = size_t(smem);
   cfg.stream = g->stream;
   int sms = 0;
