@@ -666,9 +666,13 @@ tiled_kernel(const __grid_constant__ TiledParams p,
   const int row = int(ptx::cluster_rank());
   const unsigned cid = ptx::cluster_id_x(), ncl = ptx::num_clusters_x();
   const bool exchange = p.do_degrid && p.has_model;
-  // every role that reads a ring slot releases it (one exchange warp per
-  // visibility)
-  const uint32_t empty_count = uint32_t((exchange ? kDGPer : 0) + 1 + kGR);
+  // Slot q is released by the last roles to read it.  With gridding those
+  // are the gridding warps alone: they read it after their wait on
+  // gvfull[q], which the exchange warp arrives on after its own last read,
+  // and the exchange warp started only after the degridding warps' hand-off
+  // (dgfull) that followed their last read.  Without gridding the exchange
+  // warp releases it too (the gridding warps then only wait for the copies).
+  const uint32_t empty_count = uint32_t(kGR + (p.do_grid ? 0 : 1));
 
   if (tid == 0) {
     for (int s = 0; s < kSlots; ++s) {
@@ -946,10 +950,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           if (ptx::warp_flag(abort)) continue;
           if ((lane & 3) == 0) dgpart[(b * kDG + warp) * 8 + vidx] = double(v1);
           __syncwarp();
-          if (lane == 0) {
-            ptx::mbar_arrive(&dgfull[b]);
-            ptx::mbar_arrive(&empty[s]);
-          }
+          if (lane == 0) ptx::mbar_arrive(&dgfull[b]);
           __syncwarp();
         }
       } else if (warp < kGRBase) {
@@ -958,8 +959,9 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         // degrid partial buffer q % 2 is its own).  For each of them it
         // sends this row's partials to every CTA of the cluster, waits for
         // the other rows' partials and finishes the visibility at once, so
-        // that its ring part is released as early as possible (the other
-        // exchange warp meanwhile takes the next visibility).  A remote CTA
+        // that the gridding warps can take it up (and release its ring part)
+        // as early as possible (the other exchange warp meanwhile takes the
+        // next visibility).  A remote CTA
         // sends into exchange buffer q % 8 again only for q + 8, after it
         // finished q + 6, which needed this CTA's partials of q + 6, sent
         // after this warp finished q: the buffer is never overwritten while
@@ -968,9 +970,11 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         for (int k = 0; k < ch.count; ++k, ++q) {
           if ((q & 1) != uint32_t(xw)) continue;
           {
+            // with degridding, the degridding warps' hand-off (dgfull)
+            // follows their own wait on the slot's copies and covers it
             const int s = int(q % uint32_t(kSlots));
             TT_BEGIN();
-            ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
+            if (!exchange) ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
             TT_END(1);
             if (exchange && !ptx::warp_flag(abort)) {
               const int xs = int(q % uint32_t(kXSlots));
@@ -1061,8 +1065,10 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             if (live && lane == 0 && p.do_grid) wchunk += twgt;
             __syncwarp();
             if (live && lane == 0) {
-              if (p.do_grid) ptx::mbar_arrive(&gvfull[gs]);
-              ptx::mbar_arrive(&empty[s]);
+              if (p.do_grid)
+                ptx::mbar_arrive(&gvfull[gs]);
+              else
+                ptx::mbar_arrive(&empty[s]);
             }
             __syncwarp();
             TT_END(5);
@@ -1076,13 +1082,18 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         const int gw = warp - kGRBase;
         for (int k = 0; k < ch.count; ++k, ++q) {
           const int s = int(q % uint32_t(kSlots));
-          TT_BEGIN();
-          ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
-          TT_END(1);
           if (p.do_grid) {
             const int gs = int(q % uint32_t(kSlots));
-            // the loop state needs only the descriptor: formed before the
-            // wait for the gridding values
+            // The exchange warp arrives on gvfull only after it has seen
+            // the slot's copies land (its own wait on full, or the
+            // degridding warps' hand-off that followed theirs), so this one
+            // wait also covers the slot: a wait on an mbarrier whose phase
+            // is already complete still costs ~100 cycles here.
+            TT_BEGIN();
+            ok &= ptx::mbar_wait(&gvfull[gs], (q / kSlots) & 1, abort);
+            TT_END(1);
+            // loop state from the descriptor, formed while the other
+            // gridding warps may still work on the previous visibility
             const VisGeom vg = vis_geom(descs[s]);
             int pp[N];
 #pragma unroll
@@ -1092,7 +1103,6 @@ tiled_kernel(const __grid_constant__ TiledParams p,
                 vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]),
                 ptx::smem(gtile), R, gw * 32 + lane, kGR * 32, vg.tx * vg.ty);
             TT_BEGIN();
-            ok &= ptx::mbar_wait(&gvfull[gs], (q / kSlots) & 1, abort);
             if (k > 0) ptx::named_sync(2, kGR * 32);
             TT_END(6);
             TT_BEGIN();
@@ -1109,6 +1119,11 @@ tiled_kernel(const __grid_constant__ TiledParams p,
                 grid_cells<N, MIXED, DENSE, false>(vg, pp, cur, gv);
             }
             TT_END(7);
+          } else {
+            // nothing to grid: release the slot once its copies landed
+            TT_BEGIN();
+            ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
+            TT_END(1);
           }
           __syncwarp();
           if (lane == 0) ptx::mbar_arrive(&empty[s]);
@@ -1251,11 +1266,11 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
   const int taps = std::max(cf.max_taps_x, cf.max_taps_y);
   // CF byte ring: five of the largest parts if the tiles still fit, else
   // four (more visibilities in flight when parts are smaller); the tiles
-  // take the rest.  Four is the least that cannot deadlock: an exchange warp
-  // releases visibility q only after visibility q + 2 has arrived, so the
-  // ring must take a third part while it holds any two, and an allocation
-  // that does not fit before the ring end starts over at its beginning.
-  // The deeper ring is taken only while the smaller tiles it leaves still
+  // take the rest.  Four is the least the plan takes: no role waits for a
+  // later visibility before it hands on or releases visibility q, so a
+  // smaller ring could not deadlock, but it would leave even fewer
+  // visibilities in flight than the four-part ring, the slower of the two
+  // measured.  The deeper ring is taken only while the smaller tiles it leaves still
   // hold kMinVisPerTile visibilities of the batch on average (measured: the
   // deeper ring wins at 10M visibilities on a 2048^2 grid in both forms,
   // loses at 1M in the FP64 form, whose 16-byte tiles shrink to 5x5 cells).
