@@ -32,13 +32,16 @@
 //                           the partials to every CTA of the cluster through
 //                           distributed shared memory and a remote mbarrier,
 //                           and form the prediction, residual and gridding
-//                           values (identically in every CTA), finishing
-//                           visibility q after sending those of q + 2;
+//                           values (identically in every CTA) as soon as
+//                           the other rows' partials arrive;
 //                         - 8 gridding warps add the scaled residual of one
 //                           visibility at a time into the row's
-//                           shared-memory grid tile;
-//                         - at the end of a chunk the tile is added to the
-//                           FP64 grid with red.global.add.f64, and the row's
+//                           shared-memory grid tile (mixed form: two groups
+//                           of 4 take alternate visibilities, each with a
+//                           tile of its own);
+//                         - at the end of a chunk the tile (the sum of the
+//                           groups' tiles) is added to the FP64 grid with
+//                           red.global.add.f64, and the row's
 //                           weight sum to the weights.
 // Each CF value therefore crosses HBM once per visibility, the model and grid
 // tiles once per chunk.
@@ -135,6 +138,7 @@ struct TiledParams {
   int R, T, ntx, nty;
   int ring_bytes, model_bytes;  // CF ring size (bytes, multiple of 128)
   int esize_model, esize_grid;  // bytes per tile element; 0 when unused
+  int grid_tiles;  // gridding groups, each with a grid tile (kGridTiles)
   int nplanes[4];
   int nruns[4];
   int run_plane[4][kMaxRuns];
@@ -183,7 +187,8 @@ __host__ __device__ inline int align_up(int v, int a) { return (v + a - 1) / a *
 
 __host__ __device__ inline SmemLayout smem_layout(int ring_bytes, int R,
                                                   int esize_model,
-                                                  int esize_grid) {
+                                                  int esize_grid,
+                                                  int grid_tiles) {
   SmemLayout L;
   // mbarriers full[kSlots] empty[kSlots] model xchg[kXSlots] dgfull[2]
   // dgempty[2] gvfull[kSlots] req[kSlots], then the abort flag
@@ -198,7 +203,7 @@ __host__ __device__ inline SmemLayout smem_layout(int ring_bytes, int R,
   L.ring = align_up(L.desc + kSlots * int(sizeof(TileDesc)), 1024);
   L.model = align_up(L.ring + ring_bytes, 1024);
   L.grid = align_up(L.model + R * R * esize_model, 128);
-  L.total = L.grid + R * R * esize_grid;
+  L.total = L.grid + R * R * esize_grid * grid_tiles;
   return L;
 }
 
@@ -351,6 +356,11 @@ __global__ void model_to_f32_kernel(const double2* __restrict__ in,
 
 template <bool MIXED>
 struct Form;
+
+// gridding groups, each with a grid tile of its own: two in the mixed form
+// (8-byte tiles leave room for a second one), one in the FP64 form
+template <bool MIXED>
+constexpr int kGridTiles = MIXED ? 2 : 1;
 
 template <>
 struct Form<false> {
@@ -632,7 +642,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       sm_raw + ((1024u - (ptx::smem(sm_raw) & 1023u)) & 1023u);
   // same layout the host sized the launch with (tiles absent when unused)
   const SmemLayout L =
-      smem_layout(p.ring_bytes, p.R, p.esize_model, p.esize_grid);
+      smem_layout(p.ring_bytes, p.R, p.esize_model, p.esize_grid, p.grid_tiles);
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + L.bars);
   uint64_t* empty = full + kSlots;
   uint64_t* model_bar = empty + kSlots;
@@ -667,12 +677,13 @@ tiled_kernel(const __grid_constant__ TiledParams p,
   const unsigned cid = ptx::cluster_id_x(), ncl = ptx::num_clusters_x();
   const bool exchange = p.do_degrid && p.has_model;
   // Slot q is released by the last roles to read it.  With gridding those
-  // are the gridding warps alone: they read it after their wait on
+  // are the gridding warps of the group that takes q alone: they read it after their wait on
   // gvfull[q], which the exchange warp arrives on after its own last read,
   // and the exchange warp started only after the degridding warps' hand-off
   // (dgfull) that followed their last read.  Without gridding the exchange
   // warp releases it too (the gridding warps then only wait for the copies).
-  const uint32_t empty_count = uint32_t(kGR + (p.do_grid ? 0 : 1));
+  constexpr int kGT = kGridTiles<MIXED>;
+  const uint32_t empty_count = uint32_t(kGR / kGT + (p.do_grid ? 0 : 1));
 
   if (tid == 0) {
     for (int s = 0; s < kSlots; ++s) {
@@ -859,7 +870,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
                          model_bar);
       }
       if (p.do_grid)
-        for (int i = tid; i < RR; i += kConsumers) {
+        for (int i = tid; i < RR * kGT; i += kConsumers) {
           GT z;
           z.x = 0;
           z.y = 0;
@@ -1076,11 +1087,20 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         }
       } else {
         // -------- gridding warps --------
-        // All gridding warps cover the cells of one visibility between two
-        // barriers (id 2), so footprints of consecutive visibilities that
-        // overlap are never added to the tile at the same time.
+        // The gridding warps form kGT groups: group g takes the
+        // visibilities q with q % kGT == g and adds them into a grid
+        // tile of its own, so two groups never touch the same tile.  The
+        // warps of a group cover the cells of one visibility between two
+        // barriers (id 2 + g), so footprints of the group's consecutive
+        // visibilities that overlap are never added at the same time.
         const int gw = warp - kGRBase;
+        constexpr int gper = kGR / kGT;  // warps per group
+        const int grp = gw / gper;
+        const uint32_t mytile =
+            ptx::smem(gtile) + uint32_t(grp * RR) * uint32_t(sizeof(GT));
+        bool first = true;  // the group's first visibility of the chunk
         for (int k = 0; k < ch.count; ++k, ++q) {
+          if (int(q % uint32_t(kGT)) != grp) continue;
           const int s = int(q % uint32_t(kSlots));
           if (p.do_grid) {
             const int gs = int(q % uint32_t(kSlots));
@@ -1100,10 +1120,16 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             for (int v = 0; v < N; ++v)
               pp[v] = int(int8_t((vg.pos_w ? gpk[1] : gpk[0]) >> (8 * v)));
             const GridCursor<N> cur = grid_prepare<N, MIXED>(
-                vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]),
-                ptx::smem(gtile), R, gw * 32 + lane, kGR * 32, vg.tx * vg.ty);
+                vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]), mytile, R,
+                (gw % gper) * 32 + lane, gper * 32, vg.tx * vg.ty);
             TT_BEGIN();
-            if (k > 0) ptx::named_sync(2, kGR * 32);
+            if (!first) {
+              if constexpr (kGT == 1)
+                ptx::named_sync(2, gper * 32);
+              else
+                ptx::named_sync(2 + grp, gper * 32);
+            }
+            first = false;
             TT_END(6);
             TT_BEGIN();
             if (!ptx::warp_flag(abort)) {
@@ -1136,11 +1162,18 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         for (int i = tid; i < RR; i += kConsumers) {
           const int gx = x0 + i % R, gy = y0 + i / R;
           if (gx < p.nx && gy < p.ny) {
-            const GT v = gtile[i];
-            if (v.x != 0 || v.y != 0) {
+            // the gridding groups' tiles, summed in FP64
+            double vx = 0.0, vy = 0.0;
+#pragma unroll
+            for (int t = 0; t < kGT; ++t) {
+              const GT v = gtile[t * RR + i];
+              vx += double(v.x);
+              vy += double(v.y);
+            }
+            if (vx != 0 || vy != 0) {
               double2* dst = plane + size_t(gy) * p.nx + gx;
-              atomicAdd(&dst->x, double(v.x));
-              atomicAdd(&dst->y, double(v.y));
+              atomicAdd(&dst->x, vx);
+              atomicAdd(&dst->y, vy);
             }
           }
         }
@@ -1283,12 +1316,15 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
     pl.why = "the CF ring must hold at least four parts";
     return pl;
   }
+  // grid tiles: one per gridding group
+  const int gt = mixed ? kGridTiles<true> : kGridTiles<false>;
   for (int m = m_hi; m >= m_lo; --m) {
     const int rb = m * part;
-    const SmemLayout L0 = smem_layout(rb, 0, em, eg);
+    const SmemLayout L0 = smem_layout(rb, 0, em, eg, gt);
     const int left = budget - L0.total - 1024 - 1024;
     if (left <= 0) continue;
-    int R = (em + eg) > 0 ? int(std::sqrt(double(left) / double(em + eg))) : 128;
+    const int per_cell = em + eg * gt;
+    int R = per_cell > 0 ? int(std::sqrt(double(left) / double(per_cell))) : 128;
     R = std::min(R, 128) & ~1;
     if (R - taps + 1 < 4) continue;
     if (!fixed && m > m_lo) {
@@ -1308,7 +1344,7 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
   pl.T = pl.R - taps + 1;
   pl.K = g->tiled_chunk_vis > 0 ? g->tiled_chunk_vis
                                 : (mixed ? kChunkVisMixed : kChunkVisFP64);
-  pl.smem = smem_layout(pl.ring_bytes, pl.R, em, eg).total + 1024;
+  pl.smem = smem_layout(pl.ring_bytes, pl.R, em, eg, gt).total + 1024;
   if (em > 0 && (2 * size_t(g->grid_size[0]) * (mixed ? 4 : 8)) % 16 != 0) {
     pl.why = "model row pitch not a 16-byte multiple";
     return pl;
@@ -1325,6 +1361,7 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
   p.model_bytes = pl.R * pl.R * esize;
   p.esize_model = em;
   p.esize_grid = eg;
+  p.grid_tiles = gt;
   p.do_degrid = do_degrid;
   p.do_grid = do_grid;
   p.update_weights = (flags & HPGB_UPDATE_GRID_WEIGHTS) != 0;
@@ -1340,8 +1377,10 @@ Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
   using GT = typename Form<MIXED>::grid_t;
   // the kernel places its tiles with these sizes; they must match the form
   if ((p.esize_model != 0 && p.esize_model != int(sizeof(MT))) ||
+      p.grid_tiles != kGridTiles<MIXED> ||
       (p.esize_grid != 0 && p.esize_grid != int(sizeof(GT))) ||
-      smem_layout(p.ring_bytes, p.R, p.esize_model, p.esize_grid).total +
+      smem_layout(p.ring_bytes, p.R, p.esize_model, p.esize_grid,
+                  p.grid_tiles).total +
               1024 > smem)
     return Status::err(HPGB_ERROR_OTHER, "tiled kernel layout mismatch");
   if ((p.do_degrid && p.has_model && p.esize_model == 0) ||
