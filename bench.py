@@ -261,7 +261,7 @@ def main():
     import torch
     import torch.distributed as dist
     import hpg_b200
-    from hpg_b200 import CFArray, Gridder, workloads
+    from hpg_b200 import CFArray, Gridder, abi, workloads
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -391,17 +391,26 @@ def main():
             g.set_precision(hpg_b200.PRECISION_MIXED if form == "mixed"
                             else hpg_b200.PRECISION_FP64)
             g.reset_grid()
-            step_device()
+            # the same step, returning the residual visibilities into a copy
+            # of the batch
+            dres = dvis.clone()
+            g.degrid_grid_get_residual_visibilities(dres, on_device=True)
             g.fence()
-            grids[form] = (g.grid_values(), g.grid_weights())
-        gf, wf = grids["fp64"]
-        gm, wm = grids["mixed"]
+            res = np.frombuffer(dres.cpu().numpy().tobytes(),
+                                abi.visdata_dtype(4))["vis"]
+            grids[form] = (g.grid_values(), g.grid_weights(), res)
+            del dres
+        gf, wf, rf = grids["fp64"]
+        gm, wm, rm = grids["mixed"]
         mixed_err = {
             "grid_rel": float(np.linalg.norm((gm - gf).ravel()) /
                               np.linalg.norm(gf.ravel())),
             "weights_rel": float(np.linalg.norm(wm - wf) / np.linalg.norm(wf)),
+            "residual_vis_rel": float(
+                np.linalg.norm((rm.astype(np.complex128) - rf).ravel()) /
+                np.linalg.norm(rf.astype(np.complex128).ravel())),
         }
-        del grids, gf, gm
+        del grids, gf, gm, rf, rm
 
     cpu = None
     if cpu_wl is not None:
