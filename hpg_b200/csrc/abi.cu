@@ -309,6 +309,13 @@ int hpgb_destroy(hpgb_gridder* g) {
       cudaEventDestroy(e.first);
       cudaEventDestroy(e.second);
     }
+    if (g->copy_stream) {
+      cudaStreamSynchronize(g->copy_stream);
+      cudaStreamDestroy(g->copy_stream);
+    }
+    if (g->staged_copied) cudaEventDestroy(g->staged_copied);
+    for (cudaEvent_t e : g->staged_free)
+      if (e) cudaEventDestroy(e);
     cudaStream_t s = g->stream;
     delete g;  // DevBuf destructors free device memory
     if (s) cudaStreamDestroy(s);
@@ -429,6 +436,16 @@ int hpgb_set_model(hpgb_gridder* g, const void* values, const unsigned ext[4],
   });
 }
 
+// copy stream and events of the staged host-batch path, made on first use
+static Status ensure_staging(hpgb_gridder* g) {
+  if (g->copy_stream) return Status::ok();
+  HPGB_CUDA_TRY(cudaEventCreateWithFlags(&g->staged_copied, cudaEventDisableTiming));
+  for (int b = 0; b < 2; ++b)
+    HPGB_CUDA_TRY(cudaEventCreateWithFlags(&g->staged_free[b], cudaEventDisableTiming));
+  HPGB_CUDA_TRY(cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking));
+  return Status::ok();
+}
+
 int hpgb_grid_visibilities(hpgb_gridder* g, const void* vis, size_t n,
                            unsigned npol, unsigned flags, int vis_on_device,
                            void* returned) {
@@ -456,33 +473,69 @@ int hpgb_grid_visibilities(hpgb_gridder* g, const void* vis, size_t n,
     HPGB_CUDA_TRY(cudaSetDevice(g->device));
     const size_t rec = visdata_size(npol);
     const size_t bytes = n * rec;
-    HPGB_TRY(g->vb.vis.reserve(g->max_batch * rec));
+    // A host batch outside a stream capture is copied on the copy stream
+    // into the staging buffer not used by the previous call, so that the
+    // copy overlaps the previous call's work (the work on the gridder's
+    // stream waits for it).  Device batches and captured calls copy into
+    // vb.vis on the gridder's stream.
+    bool staged = false;
+    if (!vis_on_device) {
+      cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+      HPGB_CUDA_TRY(cudaStreamIsCapturing(g->stream, &cap));
+      staged = cap == cudaStreamCaptureStatusNone;
+    }
+    const int b = g->staged_next;
+    void* dvis = nullptr;
+    cudaStream_t cs = g->stream;
+    if (staged) {
+      HPGB_TRY(ensure_staging(g));
+      HPGB_TRY(g->vb.staged[b].reserve(g->max_batch * rec));
+      dvis = g->vb.staged[b].ptr;
+      cs = g->copy_stream;
+      // the buffer's batch of two calls ago must be done with it
+      HPGB_CUDA_TRY(cudaStreamWaitEvent(cs, g->staged_free[b], 0));
+    } else {
+      HPGB_TRY(g->vb.vis.reserve(g->max_batch * rec));
+      dvis = g->vb.vis.ptr;
+    }
     // the copy is queued first, so that checking the indexes of host
     // records overlaps the transfer; a batch that fails the check is
     // copied (the call waits for that copy, the caller may free its
     // buffer on return) but never gridded
     HPGB_CUDA_TRY(cudaMemcpyAsync(
-        g->vb.vis.ptr, vis, bytes,
-        vis_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-        g->stream));
+        dvis, vis, bytes,
+        vis_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, cs));
+    if (staged) {
+      HPGB_CUDA_TRY(cudaEventRecord(g->staged_copied, cs));
+      HPGB_CUDA_TRY(cudaStreamWaitEvent(g->stream, g->staged_copied, 0));
+    }
+    Status st = Status::ok();
     if (!vis_on_device) {
-      Status v = validate_indexes(g, vis, n);
-      if (!v) {
-        cudaStreamSynchronize(g->stream);
-        return v;
+      st = validate_indexes(g, vis, n);
+      if (!st) cudaStreamSynchronize(g->stream);
+    }
+    if (st) st = grid_batch(g, dvis, n, flags);
+    if (st && (flags & HPGB_RETURN_VISIBILITIES)) {
+      const cudaError_t e = cudaMemcpyAsync(
+          returned, dvis, bytes,
+          vis_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+          g->stream);
+      if (e != cudaSuccess) {
+        st = Status::err(HPGB_ERROR_OTHER, cudaGetErrorString(e));
+      } else {
+        g->pending_dst = returned;
+        g->pending_bytes = bytes;
+        g->pending_on_device = vis_on_device != 0;
       }
     }
-    HPGB_TRY(grid_batch(g, g->vb.vis.ptr, n, flags));
-    if (flags & HPGB_RETURN_VISIBILITIES) {
-      HPGB_CUDA_TRY(cudaMemcpyAsync(
-          returned, g->vb.vis.ptr, bytes,
-          vis_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-          g->stream));
-      g->pending_dst = returned;
-      g->pending_bytes = bytes;
-      g->pending_on_device = vis_on_device != 0;
+    if (staged) {
+      // everything queued that reads the buffer precedes this record
+      const cudaError_t e = cudaEventRecord(g->staged_free[b], g->stream);
+      if (e != cudaSuccess && st)
+        st = Status::err(HPGB_ERROR_OTHER, cudaGetErrorString(e));
+      g->staged_next = b ^ 1;
     }
-    return Status::ok();
+    return st;
   });
 }
 

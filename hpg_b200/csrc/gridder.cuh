@@ -46,6 +46,10 @@ struct VisBuffers {
   // tiled path: sorted work description
   DevBuf keys, keys_alt, order, order_alt, sort_tmp, buckets, items, counters;
   DevBuf prep;      // per-visibility prepared records (sorted order)
+  // host batches outside a stream capture: two staging buffers, used in
+  // turn, so that one call's host->device copy overlaps the previous call's
+  // work
+  DevBuf staged[2];
 };
 
 struct hpgb_gridder_impl;
@@ -70,6 +74,13 @@ struct hpgb_gridder {
   int precision = HPGB_PRECISION_FP64;
 
   cudaStream_t stream = nullptr;
+  // copies of host batches into vb.staged[staged_next]: on copy_stream,
+  // after the buffer's previous batch is done with it (staged_free[b],
+  // recorded on `stream`); `stream` waits for the copy (staged_copied)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t staged_copied = nullptr;
+  cudaEvent_t staged_free[2] = {nullptr, nullptr};
+  int staged_next = 0;
 
   hpgb::DevBuf grid;      // double2 [cube][mrow][y][x]
   hpgb::DevBuf weights;   // double  [cube][mrow]

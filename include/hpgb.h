@@ -209,7 +209,12 @@ HPGB_API int hpgb_set_model(hpgb_gridder* gridder, const void* values,
 
 /* State::grid_visibilities (src/hpg_runtime.hpp:144-151, impl :965-1188).
  * visibilities: num_visibilities hpgb_visdataN records with N =
- * num_polarizations, in host memory (vis_on_device 0) or device memory.
+ * num_polarizations, in host memory (vis_on_device 0) or device memory;
+ * host records are copied asynchronously (from pinned memory the copy may
+ * still run after the call returns), so they must stay unchanged until the
+ * next hpgb_fence().  A host batch's copy runs on a stream of its own, into
+ * one of two staging buffers taken in turn, so that it overlaps the work of
+ * the previous call.
  * flags: hpgb_grid_flags.  When HPGB_RETURN_VISIBILITIES is set, the
  * predicted or residual records are written to returned (host or device
  * memory, same kind as the input; may equal visibilities) and are valid after

@@ -202,7 +202,8 @@ def test_degrid_grid_parity(gpu, oracle_lib, grad, kernel, precision):
 
 @pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED],
                          ids=["fp64", "mixed"])
-@pytest.mark.parametrize("ring_parts,chunk", [(4, 64), (6, 0), (5, 7)])
+@pytest.mark.parametrize("ring_parts,chunk", [(4, 64), (6, 0), (5, 7), (4, 1),
+                                             (5, 2)])
 def test_tiled_plan_overrides(gpu, oracle_lib, precision, ring_parts, chunk):
     """Every ring depth and tile-pass length the plan accepts gives the same
     results: small chunks cross many tile flushes, a deep ring keeps many
@@ -323,6 +324,36 @@ def test_multi_batch_and_cubes(gpu, oracle_lib, kernel, precision):
         vis["grid_cube"] = rng.integers(0, 3, len(vis))
         g.degrid_grid_visibilities(vis)
         o.grid_visibilities(vis, do_degrid=True)
+    assert rel_norm(g.grid_values(), o.grid) <= 1e-6
+    np.testing.assert_allclose(g.grid_weights(), o.weights, rtol=1e-12)
+
+
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED],
+                         ids=["fp64", "mixed"])
+def test_pinned_batches_back_to_back(gpu, oracle_lib, precision):
+    """Host batches in pinned memory, four calls without a fence between
+    them: each call's copy runs while the previous call's work is on the
+    device (two staging buffers in turn); the last call returns residuals."""
+    import torch
+    cfg = small_full_pol(4000, grad=0.3, seed=17)
+    g, o = make_pair(cfg, oracle_lib, max_batch=2000, precision=precision,
+                     kernel="tiled")
+    halves = [cfg["vis"][:2000], cfg["vis"][2000:]]
+    pinned = []
+    for h in halves:
+        t = torch.from_numpy(np.frombuffer(h.tobytes(), np.uint8).copy()).pin_memory()
+        pinned.append(t.numpy().view(h.dtype))
+    for k in range(3):
+        g.degrid_grid_visibilities(pinned[k % 2])
+        o.grid_visibilities(halves[k % 2], do_degrid=True)
+    fut = g.degrid_grid_get_residual_visibilities(pinned[1])
+    exp = o.grid_visibilities(halves[1], do_degrid=True, return_vis=True)
+    g.fence()
+    res = fut.get()
+    if precision == abi.PRECISION_FP64:
+        assert np.mean(np.all(res["vis"] == exp["vis"], axis=1)) > 0.99
+    else:
+        assert rel_norm(res["vis"], exp["vis"]) <= 1e-6
     assert rel_norm(g.grid_values(), o.grid) <= 1e-6
     np.testing.assert_allclose(g.grid_weights(), o.weights, rtol=1e-12)
 
