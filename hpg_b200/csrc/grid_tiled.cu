@@ -24,7 +24,9 @@
 //                           mbarrier completion (16 visibilities in flight
 //                           at most, bounded by the ring's bytes);
 //                         - the model tile of row r is loaded once per chunk
-//                           with a 3-D TMA tensor copy;
+//                           with a 3-D TMA tensor copy (FP64 form: the next
+//                           chunk's as soon as the degridding warps are
+//                           done with the current one);
 //                         - 8 degridding warps in two groups of 4 take
 //                           alternate visibilities: partial sums of row r
 //                           over the footprint, reduced per warp;
@@ -853,6 +855,25 @@ tiled_kernel(const __grid_constant__ TiledParams p,
     uint32_t q = 0;
     uint32_t model_phase = 0;
     TT_DECL(10);
+    // the model tile of this cluster's chunk cc, copied by one thread.  FP64
+    // form: the first chunk's here, each next one's as soon as the
+    // degridding warps (its only readers) are done with the current one, so
+    // the copy runs while the other roles finish the chunk and flush the
+    // grid tile.  Mixed form: at the start of each chunk (loading early
+    // there costs registers the mixed cell loops need: measured slower).
+    constexpr bool kEarlyModel = !MIXED;
+    auto load_model = [&](unsigned cc) {
+      const int t = p.chunks[cc].tile;
+      const int mx = (t % p.ntx) * p.T, my = ((t / p.ntx) % p.nty) * p.T;
+      const int mc = t / (p.ntx * p.nty);
+      // earlier generic-proxy reads of the tile precede this async write
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      ptx::mbar_expect_tx(model_bar, uint32_t(p.model_bytes));
+      ptx::tma_load_3d(mtile, &model_map, 2 * mx, my, mc * p.nrow + row,
+                       model_bar);
+    };
+    if (kEarlyModel && exchange && tid == 0 && cid < nchunks && !*abort)
+      load_model(cid);
     for (unsigned c = cid; c < nchunks; c += ncl) {
       const Chunk ch = p.chunks[c];
       const int tile = ch.tile;
@@ -862,13 +883,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       const int x0 = tx * p.T, y0 = ty * p.T;
       TT_BEGIN();
       ptx::named_sync(1, kConsumers);
-      if (exchange && tid == 0 && !*abort) {
-        // earlier generic-proxy reads of the tile precede this async write
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        ptx::mbar_expect_tx(model_bar, uint32_t(p.model_bytes));
-        ptx::tma_load_3d(mtile, &model_map, 2 * x0, y0, cube * p.nrow + row,
-                         model_bar);
-      }
+      if (!kEarlyModel && exchange && tid == 0 && !*abort) load_model(c);
       if (p.do_grid)
         for (int i = tid; i < RR * kGT; i += kConsumers) {
           GT z;
@@ -963,6 +978,12 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           __syncwarp();
           if (lane == 0) ptx::mbar_arrive(&dgfull[b]);
           __syncwarp();
+        }
+        if constexpr (kEarlyModel) {
+          // every degridding warp is done with this chunk's model tile
+          ptx::named_sync(4, kDG * 32);
+          if (exchange && tid == 0 && c + ncl < nchunks && !*abort)
+            load_model(c + ncl);
         }
       } else if (warp < kGRBase) {
         // -------- exchange warps --------
