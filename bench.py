@@ -167,6 +167,11 @@ def kernel_traffic(form, nvis, grid_elems):
     return TRAFFIC_PER_VIS_FP64 * nvis + grid_elems * (16 + 32)
 
 
+def workload_name(args):
+    return (f"full-pol degrid+grid {args.grid}x{args.grid}x4, 8 CF groups "
+            f"(supports 8-32, os {args.oversampling}), dense 4x4 Mueller")
+
+
 def taps_of(supports):
     return [s + 1 if s % 2 == 0 else s for s in supports]
 
@@ -238,8 +243,7 @@ def run_reference(args, rank):
         "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "full-pol degrid+grid 2048x2048x4, 8 CF groups "
-                               "(supports 8-32, os 128), dense 4x4 Mueller",
+        "config": {"workload": workload_name(args),
                    "nvis": args.nvis, "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads,
                          "kind": "port",
@@ -462,8 +466,7 @@ def main():
             "dtype": "f64" if forms[0] == "fp64" else "f32-mixed",
             "data": "synthetic",
             "config": {
-                "workload": "full-pol degrid+grid 2048x2048x4, 8 CF groups "
-                            "(supports 8-32, os 128), dense 4x4 Mueller",
+                "workload": workload_name(args),
                 "nvis": args.nvis, "grid": list(wl["grid_size"]),
                 "precision": forms[0],
                 "l2": "inputs larger than L2 (CF 10 GB, visibilities 1.2 GB)",
