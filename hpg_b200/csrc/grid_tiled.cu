@@ -679,11 +679,12 @@ tiled_kernel(const __grid_constant__ TiledParams p,
   const unsigned cid = ptx::cluster_id_x(), ncl = ptx::num_clusters_x();
   const bool exchange = p.do_degrid && p.has_model;
   // Slot q is released by the last roles to read it.  With gridding those
-  // are the gridding warps of the group that takes q alone: they read it after their wait on
-  // gvfull[q], which the exchange warp arrives on after its own last read,
-  // and the exchange warp started only after the degridding warps' hand-off
-  // (dgfull) that followed their last read.  Without gridding the exchange
-  // warp releases it too (the gridding warps then only wait for the copies).
+  // are the warps of the gridding group that takes q alone: they read it
+  // after their wait on gvfull[q], which the exchange warp arrives on after
+  // its own last read, and the exchange warp started only after the
+  // degridding warps' hand-off (dgfull) that followed their last read.
+  // Without gridding the exchange warp releases it too (the gridding warps
+  // then only wait for the copies).
   constexpr int kGT = kGridTiles<MIXED>;
   const uint32_t empty_count = uint32_t(kGR / kGT + (p.do_grid ? 0 : 1));
 
