@@ -172,6 +172,14 @@ def workload_name(args):
             f"(supports 8-32, os {args.oversampling}), dense 4x4 Mueller")
 
 
+def config_of(args, world, precision):
+    """The workload's config object, the same in both arms."""
+    return {"workload": workload_name(args), "nvis": args.nvis,
+            "grid": [args.grid, args.grid, 4, 1], "precision": precision,
+            "l2": "inputs larger than L2 (CF 10 GB, visibilities 1.2 GB)",
+            "parallelism": f"replicas x{world}"}
+
+
 def taps_of(supports):
     return [s + 1 if s % 2 == 0 else s for s in supports]
 
@@ -195,9 +203,46 @@ def cpu_baseline(wl, target_s, nthreads=None):
     dt = time.perf_counter() - t0
     n2 = int(min(len(vis) - n, max(n, target_s / max(dt / n, 1e-9))))
     t0 = time.perf_counter()
-    o.grid_visibilities(vis[n:n + n2], do_degrid=True, nthreads=nthreads)
+    res = o.grid_visibilities(vis[n:n + n2], do_degrid=True, return_vis=True,
+                              nthreads=nthreads)
     dt2 = time.perf_counter() - t0
-    return n2 / dt2 / 1e6, n2, dt2, nthreads
+    # what the oracle computed on the sample: the parity check of the
+    # device against it grids the same n + n2 visibilities
+    oracle_out = dict(n_warm=n, n_sample=n2, residuals=res["vis"],
+                      grid=o.grid, weights=o.weights)
+    return n2 / dt2 / 1e6, n2, dt2, nthreads, oracle_out
+
+
+def device_parity(g, vis, ref, form):
+    """The device's degrid+grid of the CPU-baseline sample (a fresh grid,
+    the same n_warm + n_sample visibilities) against the oracle's results:
+    relative norm errors of the grid, the weights and the residual
+    visibilities, and the fraction of bit-exact residuals."""
+    from hpg_b200 import abi
+    g.reset_grid()
+    nw, ns = ref["n_warm"], ref["n_sample"]
+    g.degrid_grid_visibilities(vis[:nw])
+    fut = g.degrid_grid_get_residual_visibilities(vis[nw:nw + ns])
+    g.fence()
+    res = fut.get()["vis"]
+    grid, wgt = g.grid_values(), g.grid_weights()
+
+    def rel(a, b):
+        return float(np.linalg.norm((a - b).ravel()) /
+                     np.linalg.norm(b.ravel()))
+    out = {"visibilities": nw + ns,
+           "grid_rel": rel(grid, ref["grid"]),
+           "weights_rel": rel(wgt, ref["weights"]),
+           "residual_rel": rel(res.astype(np.complex128),
+                               ref["residuals"].astype(np.complex128)),
+           "residual_bit_exact": float(np.mean(np.all(
+               res == ref["residuals"], axis=1)))}
+    tol = 1e-6
+    out["within_tolerance"] = bool(out["grid_rel"] <= tol and
+                                   out["residual_rel"] <= tol and
+                                   out["weights_rel"] <= 1e-12)
+    del abi
+    return out
 
 
 def run_reference(args, rank):
@@ -243,8 +288,8 @@ def run_reference(args, rank):
         "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": workload_name(args),
-                   "nvis": args.nvis, "parallelism": "host threads"},
+        "config": config_of(args, args.gpus, "mixed"
+                            if args.precision in ("both", "mixed") else "fp64"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads,
                          "kind": "port",
                          "sample": f"{n_step} visibilities per step of the "
@@ -403,16 +448,23 @@ def main():
             clock_summary = csum
 
     head = results[forms[0]]
-    e2e_value = None
-    if not args.no_e2e:
-        g.set_precision(hpg_b200.PRECISION_MIXED if forms[0] == "mixed"
+    def use_form(form):
+        g.set_precision(hpg_b200.PRECISION_MIXED if form == "mixed"
                         else hpg_b200.PRECISION_FP64)
-        if plans.get(forms[0]):
-            g.set_tiled_plan(*plans[forms[0]])
-        e2e_steps = max(2, min(args.steps, 3))
-        run_e2e(1)
-        ms_e2e = timed(lambda: run_e2e(e2e_steps), 1)
-        e2e_value = total_vis / (ms_e2e / e2e_steps * 1e-3) / 1e6
+        g.set_tiled_plan(*(plans.get(form) or (0, 0)))
+
+    # end to end, every form: at least 10 pipelined steps, so that the first
+    # step's unoverlapped copy and the last step's drain weigh little
+    e2e_value = None
+    e2e_steps = max(10, args.steps)
+    if not args.no_e2e:
+        for form in forms:
+            use_form(form)
+            run_e2e(2)
+            ms_e2e = timed(lambda: run_e2e(e2e_steps), 1)
+            results[form]["e2e"] = total_vis / (ms_e2e / e2e_steps * 1e-3) / 1e6
+            results[form]["e2e_steps"] = e2e_steps
+        e2e_value = results[forms[0]]["e2e"]
 
     # full-size error of the mixed form against the FP64 form (one step each
     # from a zero grid; the FP64 form is checked against the CPU oracle by
@@ -446,15 +498,23 @@ def main():
         del grids, gf, gm, rf, rm
 
     cpu = None
+    parity = None
     if cpu_wl is not None:
         try:
-            v, n, dt, nt = cpu_baseline(cpu_wl, args.cpu_seconds)
+            v, n, dt, nt, oracle_out = cpu_baseline(cpu_wl, args.cpu_seconds)
             cpu = {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
                    "sample": f"{n} visibilities of the same batch "
                              f"({dt:.1f} s, threaded CPU restatement)"}
         except Exception as e:  # reported, not hidden
+            oracle_out = None
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port",
                    "sample": f"failed: {e}"}
+        # the device on the same sample, from a fresh grid, every form
+        if oracle_out is not None:
+            parity = {}
+            for form in forms:
+                use_form(form)
+                parity[form] = device_parity(g, vis, oracle_out, form)
 
     if rank == 0:
         kernel_gbs = head["kernel_gbs"]
@@ -465,12 +525,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if forms[0] == "fp64" else "f32-mixed",
             "data": "synthetic",
-            "config": {
-                "workload": workload_name(args),
-                "nvis": args.nvis, "grid": list(wl["grid_size"]),
-                "precision": forms[0],
-                "l2": "inputs larger than L2 (CF 10 GB, visibilities 1.2 GB)",
-                "parallelism": f"replicas x{world}"},
+            "config": config_of(args, world, forms[0]),
             "forms": results,
             "mixed_over_fp64": (results["mixed"]["value"] /
                                 results["fp64"]["value"]
@@ -494,6 +549,7 @@ def main():
                          "step_frac": head["step_gbs"] / peak,
                          "algorithmic_bytes_per_step": b_alg},
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clock_summary,
             "gpu_launches": head["gpu_launches"],
         }

@@ -136,6 +136,7 @@ SIGNATURES = {
     "hpgb_shift_model": ([_P, _I], _I),
     "hpgb_kernel_launches": ([_P, ctypes.POINTER(ctypes.c_uint64)], _I),
     "hpgb_set_tiled_plan": ([_P, _I, _I], _I),
+    "hpgb_last_gridding_kernel": ([_P, ctypes.POINTER(ctypes.c_int)], _I),
     "hpgb_autotune_tiled": ([_P, _P, _S, _U, _U, _I, ctypes.POINTER(_I),
                              ctypes.POINTER(_I)], _I),
     "hpgb_begin_capture": ([_P], _I),

@@ -777,12 +777,20 @@ int hpgb_kernel_launches(const hpgb_gridder* g, uint64_t* count) {
 int hpgb_set_tiled_plan(hpgb_gridder* g, int ring_parts, int chunk_vis) {
   return guarded([&]() -> Status {
     if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
-    if (ring_parts < 0 || (ring_parts > 0 && ring_parts < 4) ||
+    if (ring_parts < 0 || (ring_parts > 0 && ring_parts < 2) ||
         ring_parts > 16 || chunk_vis < 0 || chunk_vis > (1 << 20))
       return Status::err(HPGB_ERROR_OTHER,
-                         "ring_parts must be 0 or 4..16 and chunk_vis 0..2^20");
+                         "ring_parts must be 0 or 2..16 and chunk_vis 0..2^20");
     g->tiled_ring_parts = ring_parts;
     g->tiled_chunk_vis = chunk_vis;
+    return Status::ok();
+  });
+}
+
+int hpgb_last_gridding_kernel(const hpgb_gridder* g, int* kind) {
+  return guarded([&]() -> Status {
+    if (!g || !kind) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    *kind = g->last_kernel;
     return Status::ok();
   });
 }

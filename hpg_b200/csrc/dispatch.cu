@@ -13,11 +13,15 @@ Status grid_batch(hpgb_gridder* g, const void* d_vis, size_t n,
   if (g->kernel_kind != HPGB_KERNEL_DIRECT) {
     bool used = false;
     HPGB_TRY(grid_tiled(g, const_cast<void*>(d_vis), n, flags, &used));
-    if (used) return Status::ok();
+    if (used) {
+      if (n > 0) g->last_kernel = HPGB_KERNEL_TILED;
+      return Status::ok();
+    }
     if (g->kernel_kind == HPGB_KERNEL_TILED)
       return Status::err(HPGB_ERROR_OTHER,
                          "the tiled kernel cannot take this CF or grid");
   }
+  if (n > 0) g->last_kernel = HPGB_KERNEL_DIRECT;
   return grid_direct(g, d_vis, n, flags);
 }
 

@@ -408,9 +408,11 @@ __device__ __forceinline__ VisGeom vis_geom(const TileDesc& d) {
 // Footprint cells c = first, first + stride, ... with their (X, Y) and the
 // shared-memory address of their tile cell (row pitch R elements of `esize`
 // bytes), advanced without integer division: the start and the step are
-// split with the float reciprocal of taps_x, exact here because
-// c + 0.5 < 2^12 and taps_x < 128 keep the rounding error (< 5e-4) below the
-// distance of (c + 0.5) / taps_x to the nearest integer (>= 0.5 / taps_x).
+// split with the float reciprocal of taps_x, exact here because with
+// c + 0.5 < 2^14 and taps_x < 128 the two float roundings (relative error
+// < 2^-23) leave an absolute error below 2^14 / taps_x * 2^-23 < 2^-9 /
+// taps_x, under the distance of (c + 0.5) / taps_x to the nearest integer
+// (>= 0.5 / taps_x).  Footprints reach 65^2 = 4225 < 2^14 cells.
 struct CellWalk {
   int X, Y, dX, dY;
   uint32_t tile, dtile, wrap;  // tile-cell address, its step, row wrap
@@ -1321,21 +1323,24 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
   const int taps = std::max(cf.max_taps_x, cf.max_taps_y);
   // CF byte ring: five of the largest parts if the tiles still fit, else
   // four (more visibilities in flight when parts are smaller); the tiles
-  // take the rest.  Four is the least the plan takes: no role waits for a
-  // later visibility before it hands on or releases visibility q, so a
-  // smaller ring could not deadlock, but it would leave even fewer
-  // visibilities in flight than the four-part ring, the slower of the two
-  // measured.  The deeper ring is taken only while the smaller tiles it leaves still
-  // hold kMinVisPerTile visibilities of the batch on average (measured: the
-  // deeper ring wins at 10M visibilities on a 2048^2 grid in both forms,
-  // loses at 1M in the FP64 form, whose 16-byte tiles shrink to 5x5 cells).
-  constexpr int kMinRingParts = 4;
+  // take the rest.  The deeper ring is taken only while the smaller tiles it
+  // leaves still hold kMinVisPerTile visibilities of the batch on average
+  // (measured: the deeper ring wins at 10M visibilities on a 2048^2 grid in
+  // both forms, loses at 1M in the FP64 form, whose 16-byte tiles shrink to
+  // 5x5 cells).  CF slices too wide for four parts (supports up to 64 with
+  // one or two Mueller planes per row: 65^2 taps are 33 KB a plane) get a
+  // ring of three or two: no role waits for a later visibility before it
+  // hands on or releases visibility q, so any ring that holds the largest
+  // part keeps the pipeline moving; a shallower one only keeps fewer
+  // visibilities in flight, which the longer per-visibility work of wide
+  // footprints covers.  kMinRingParts is the least the plan takes.
+  constexpr int kMinRingParts = 2;
   constexpr size_t kMinVisPerTile = 32;
   const bool fixed = g->tiled_ring_parts > 0;
   const int m_hi = fixed ? g->tiled_ring_parts : 5;
   const int m_lo = fixed ? g->tiled_ring_parts : kMinRingParts;
   if (m_lo < kMinRingParts) {
-    pl.why = "the CF ring must hold at least four parts";
+    pl.why = "the CF ring must hold at least two parts";
     return pl;
   }
   // grid tiles: one per gridding group

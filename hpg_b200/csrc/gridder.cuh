@@ -89,6 +89,7 @@ struct hpgb_gridder {
   hpgb::DevBuf model32;   // float2 copy of the model for the mixed form
   bool model32_valid = false;
   int kernel_kind = HPGB_KERNEL_AUTO;
+  int last_kernel = HPGB_KERNEL_AUTO;  // kernel of the last non-empty batch
   // tiled-kernel plan overrides (0: chosen by the plan)
   int tiled_ring_parts = 0;
   int tiled_chunk_vis = 0;

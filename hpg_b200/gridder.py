@@ -386,6 +386,13 @@ class Gridder:
                                             ctypes.byref(n)))
         return ms.value, n.value
 
+    def last_gridding_kernel(self):
+        """abi.KERNEL_TILED or abi.KERNEL_DIRECT: the kernel that took the
+        last non-empty batch (abi.KERNEL_AUTO before any)."""
+        k = ctypes.c_int()
+        check(load().hpgb_last_gridding_kernel(self._h, ctypes.byref(k)))
+        return k.value
+
     def kernel_launches(self):
         """Kernels this gridder has launched so far."""
         n = ctypes.c_uint64()

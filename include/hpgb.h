@@ -352,12 +352,22 @@ HPGB_API int hpgb_kernel_launches(const hpgb_gridder* gridder,
 
 /* Tiled-kernel plan overrides, no counterpart in the reference (tuning):
  * ring_parts = number of the largest per-row CF parts the shared-memory
- * ring holds (0 or 4..16; the tile side shrinks to make room), chunk_vis = visibilities
- * per tile pass between flushes of the shared-memory grid tile; 0 keeps the
- * plan's own choice.  A plan that does not fit makes the tiled kernel
- * unusable for the batch (HPGB_KERNEL_AUTO then uses the direct kernels). */
+ * ring holds (0 or 2..16; the tile side shrinks to make room), chunk_vis =
+ * visibilities per tile pass between flushes of the shared-memory grid tile;
+ * 0 keeps the plan's own choice.  The plan's own ring holds four or five
+ * parts, or two or three for CF slices too wide for four (supports up to 64
+ * with one or two Mueller planes per grid row).  A plan that does not fit
+ * makes the tiled kernel unusable for the batch (HPGB_KERNEL_AUTO then uses
+ * the direct kernels; hpgb_last_gridding_kernel tells which ran). */
 HPGB_API int hpgb_set_tiled_plan(hpgb_gridder* gridder, int ring_parts,
                                  int chunk_vis);
+
+/* Which kernel gridded/degridded the gridder's last non-empty batch:
+ * HPGB_KERNEL_TILED or HPGB_KERNEL_DIRECT (HPGB_KERNEL_AUTO before the first
+ * batch).  No counterpart in the reference: it makes the tiled kernel's
+ * fallback to the per-visibility kernels visible to the caller. */
+HPGB_API int hpgb_last_gridding_kernel(const hpgb_gridder* gridder,
+                                       int* kind);
 
 /* Autotuner of the tiled kernel, no counterpart in the reference: runs the
  * batch (as hpgb_grid_visibilities would with these flags) once per
