@@ -88,7 +88,8 @@ def visdata_dtype(npol):
 COORDS_DTYPE = np.dtype([
     ("grid_coord", np.int32, (2,)), ("cf_major", np.int32, (2,)),
     ("cf_minor", np.int32, (2,)), ("fine_offset", np.int32, (2,)),
-    ("cf_size", np.int32, (2,)), ("pos_w", np.int32), ("in_grid", np.int32)])
+    ("cf_size", np.int32, (2,)), ("pos_w", np.int32), ("in_grid", np.int32),
+    ("grid_mueller", np.int32, (4, 4)), ("degrid_mueller", np.int32, (4, 4))])
 
 _lib = None
 
@@ -137,6 +138,10 @@ SIGNATURES = {
     "hpgb_kernel_launches": ([_P, ctypes.POINTER(ctypes.c_uint64)], _I),
     "hpgb_set_tiled_plan": ([_P, _I, _I], _I),
     "hpgb_last_gridding_kernel": ([_P, ctypes.POINTER(ctypes.c_int)], _I),
+    "hpgb_set_tiled_plan_ex": ([_P, ctypes.c_void_p], _I),
+    "hpgb_set_wait_limit": ([_P, ctypes.c_double], _I),
+    "hpgb_debug_withhold_copy": ([_P, ctypes.c_longlong], _I),
+    "hpgb_get_tiled_plan": ([_P, ctypes.c_void_p], _I),
     "hpgb_autotune_tiled": ([_P, _P, _S, _U, _U, _I, ctypes.POINTER(_I),
                              ctypes.POINTER(_I)], _I),
     "hpgb_begin_capture": ([_P], _I),
@@ -148,6 +153,16 @@ SIGNATURES = {
                                 ctypes.POINTER(ctypes.c_uint64)], _I),
     "hpgb_debug_coords": ([_P, _P, _S, _U, _P], _I),
 }
+
+
+class TiledPlan(ctypes.Structure):
+    """hpgb_tiled_plan (include/hpgb.h): 0 in a field = automatic."""
+    _fields_ = [("ring_parts", ctypes.c_int), ("chunk_vis", ctypes.c_int),
+                ("tile_side", ctypes.c_int), ("compensated", ctypes.c_int)]
+
+
+COMPENSATED_OFF = 1
+COMPENSATED_ON = 2
 
 
 def load(path=LIB_PATH):

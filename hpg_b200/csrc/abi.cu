@@ -781,8 +781,53 @@ int hpgb_set_tiled_plan(hpgb_gridder* g, int ring_parts, int chunk_vis) {
         ring_parts > 16 || chunk_vis < 0 || chunk_vis > (1 << 20))
       return Status::err(HPGB_ERROR_OTHER,
                          "ring_parts must be 0 or 2..16 and chunk_vis 0..2^20");
-    g->tiled_ring_parts = ring_parts;
-    g->tiled_chunk_vis = chunk_vis;
+    g->tplan = hpgb_tiled_plan{ring_parts, chunk_vis, 0, 0};
+    return Status::ok();
+  });
+}
+
+int hpgb_set_tiled_plan_ex(hpgb_gridder* g, const hpgb_tiled_plan* plan) {
+  return guarded([&]() -> Status {
+    if (!g || !plan) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    const hpgb_tiled_plan& t = *plan;
+    if (t.ring_parts < 0 || (t.ring_parts > 0 && t.ring_parts < 2) ||
+        t.ring_parts > 16 || t.chunk_vis < 0 || t.chunk_vis > (1 << 20))
+      return Status::err(HPGB_ERROR_OTHER,
+                         "ring_parts must be 0 or 2..16 and chunk_vis 0..2^20");
+    if (t.tile_side < 0 || t.tile_side > 128 || (t.tile_side & 1))
+      return Status::err(HPGB_ERROR_OTHER,
+                         "tile_side must be 0 or an even number up to 128");
+    if (t.compensated < 0 || t.compensated > HPGB_COMPENSATED_ON)
+      return Status::err(HPGB_ERROR_OTHER, "compensated takes 0, 1 or 2");
+    g->tplan = t;
+    return Status::ok();
+  });
+}
+
+int hpgb_get_tiled_plan(const hpgb_gridder* g, hpgb_tiled_plan* plan) {
+  return guarded([&]() -> Status {
+    if (!g || !plan) return Status::err(HPGB_ERROR_OTHER, "null argument");
+    *plan = g->tplan;
+    return Status::ok();
+  });
+}
+
+int hpgb_set_wait_limit(hpgb_gridder* g, double seconds) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    if (!(seconds >= 1e-4 && seconds <= 60.0))
+      return Status::err(HPGB_ERROR_OTHER, "wait limit must be 1e-4..60 s");
+    g->wait_limit_ns = static_cast<unsigned long long>(seconds * 1e9);
+    return Status::ok();
+  });
+}
+
+int hpgb_debug_withhold_copy(hpgb_gridder* g, long long visibility) {
+  return guarded([&]() -> Status {
+    if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    if (visibility < -1)
+      return Status::err(HPGB_ERROR_OTHER, "visibility position must be >= -1");
+    g->withhold_vis = visibility;
     return Status::ok();
   });
 }

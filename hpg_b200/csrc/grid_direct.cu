@@ -237,6 +237,13 @@ __global__ void coords_kernel(const VisData<N>* vis, size_t n, GridGeom g,
   }
   o.pos_w = vc.pos_w;
   o.in_grid = vc.in_grid;
+  const int(*gm)[4] = vc.pos_w ? g.mt.m : g.mt.c;
+  const int(*dm)[4] = vc.pos_w ? g.mt.c : g.mt.m;
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) {
+      o.grid_mueller[r][c] = gm[r][c];
+      o.degrid_mueller[r][c] = dm[r][c];
+    }
 }
 
 template <int N>

@@ -69,12 +69,9 @@
 
 #include "gridder.cuh"
 #include "ptx.cuh"
+#include "tiles.cuh"
 
 namespace hpgb {
-
-#ifdef HPGB_TILED_TIMERS
-unsigned long long* g_tiled_timers = nullptr;
-#endif
 
 namespace {
 
@@ -104,43 +101,17 @@ constexpr int kThreadsTiled = kConsumers + 32 * kProducers;
 constexpr int kSlots = 16;  // descriptor slots (visibilities in flight)
 constexpr int kChunkVisFP64 = 2048;
 constexpr int kChunkVisMixed = 256;
+// compensated tiles accumulate without FP32 error: longer passes
+constexpr int kChunkVisMixedComp = 2048;
 constexpr int kMaxRuns = 8;
-
-struct alignas(16) TileDesc {
-  int32_t index;         // visibility index in the batch
-  int16_t cx, cy;        // footprint origin relative to the tile region
-  uint8_t taps_x, taps_y, flags, pad0;
-  int32_t pstride;       // CF plane stride (float2 elements)
-  double2 phasor;        // cphase(phase)
-  double phi0[2], dphi[2];
-  float2 vals[4];
-  float weights[4];
-  double2 wfac[4];       // conj(phasor) / normaliser, per polarization
-  double twgt[4];        // grid weight increment per grid row
-  float2 gvis[4];        // values scaled for gridding (used without degrid)
-  float inv_tx;          // 1 / taps_x, rounded to float
-  int32_t pad1[3];
-};
-static_assert(sizeof(TileDesc) == 256, "TileDesc is one 256-byte bulk copy");
-
-enum : uint8_t { kPosW = 1, kScreen = 2 };
-
-struct SliceRef {
-  long long off;  // float2 offset of the slice in the CF region
-  int pstride;
-  int ncell;
-};
-
-struct Chunk {
-  int tile, start, count, pad;
-};
 
 struct TiledParams {
   int nx, ny, nrow, ncube;
   int R, T, ntx, nty;
   int ring_bytes, model_bytes;  // CF ring size (bytes, multiple of 128)
   int esize_model, esize_grid;  // bytes per tile element; 0 when unused
-  int grid_tiles;  // gridding groups, each with a grid tile (kGridTiles)
+  int grid_tiles;  // grid tiles: one per gridding group, two when compensated
+  int compensated;  // mixed form: high/low tile pairs updated by two-sum
   int nplanes[4];
   int nruns[4];
   int run_plane[4][kMaxRuns];
@@ -159,27 +130,12 @@ struct TiledParams {
   unsigned char* records;  // VisData<N> records (values written back)
   int rec_stride;
   unsigned* status;
-  unsigned long long* timers;  // per-CTA phase cycle counters (timer builds)
+  unsigned long long wait_limit_ns;  // bound of every wait in the kernel
+  // test hook: CTA 0 never issues the copies of this visibility (its ring
+  // position in CTA 0's sequence), so that the waits for them run out; -1:
+  // none
+  long long withhold_vis;
 };
-
-// Phase timers: compiled in only with -DHPGB_TILED_TIMERS (measurement
-// builds); they record clock64() intervals per CTA, nothing else changes.
-#ifdef HPGB_TILED_TIMERS
-#define TT_DECL(n) unsigned long long tt_[n] = {0}; long long tt0_ = 0
-#define TT_BEGIN() tt0_ = clock64()
-#define TT_END(i) tt_[i] += (unsigned long long)(clock64() - tt0_)
-#define TT_STORE(base, n)                                              \
-  for (int i_ = 0; i_ < (n); ++i_)                                     \
-    if (p.timers) atomicAdd(&p.timers[(base) + i_], tt_[i_])
-#define TT_PUT(slot, i) \
-  if (p.timers) atomicAdd(&p.timers[blockIdx.x * 16 + (slot)], tt_[i])
-#else
-#define TT_PUT(slot, i)
-#define TT_DECL(n)
-#define TT_BEGIN()
-#define TT_END(i)
-#define TT_STORE(base, n)
-#endif
 
 struct SmemLayout {
   int bars, xbuf, wred, bcast, slots, desc, ring, model, grid, total;
@@ -195,13 +151,16 @@ __host__ __device__ inline SmemLayout smem_layout(int ring_bytes, int R,
   // mbarriers full[kSlots] empty[kSlots] model xchg[kXSlots] dgfull[2]
   // dgempty[2] gvfull[kSlots] req[kSlots], then the abort flag
   L.bars = 0;
-  L.xbuf = align_up((4 * kSlots + kXSlots + 5) * 8 + 8, 16);  // [kXSlots][4 rows][4 pol] complex double
+  // + the WaitCtl block (abort flag, wait limit)
+  L.xbuf = align_up((4 * kSlots + kXSlots + 5) * 8 + int(sizeof(ptx::WaitCtl)),
+                    16);  // [kXSlots][4 rows][4 pol] complex double
   L.wred = L.xbuf + kXSlots * 4 * 4 * 16;  // [2][kDG][8] double (degrid partials)
   L.bcast = L.wred + 2 * kDG * 8 * 8; // [kSlots][4] float2 (gridding values)
   // slot_end[kSlots] u64, req_src[kSlots] i64, ring_off[kSlots] int,
-  // req_off[kSlots] int, req_pst[kSlots] int, req_desc[kSlots] int
+  // req_off[kSlots] int, req_pst[kSlots] int, req_desc[kSlots] int,
+  // issued[kSlots] int
   L.slots = L.bcast + kSlots * 4 * 8;
-  L.desc = align_up(L.slots + kSlots * (8 + 8 + 4 + 4 + 4 + 4), 128);
+  L.desc = align_up(L.slots + kSlots * (8 + 8 + 4 + 4 + 4 + 4 + 4), 128);
   L.ring = align_up(L.desc + kSlots * int(sizeof(TileDesc)), 1024);
   L.model = align_up(L.ring + ring_bytes, 1024);
   L.grid = align_up(L.model + R * R * esize_model, 128);
@@ -211,10 +170,6 @@ __host__ __device__ inline SmemLayout smem_layout(int ring_bytes, int R,
 
 // ---------------------------------------------------------------------------
 // preparation kernels
-
-struct TileGeom {
-  int T, ntx, nty, ntiles;  // ntiles = ncube * nty * ntx (also the invalid key)
-};
 
 template <int N>
 __global__ void tile_keys_kernel(const VisData<N>* vis, size_t n, GridGeom g,
@@ -363,6 +318,12 @@ struct Form;
 // (8-byte tiles leave room for a second one), one in the FP64 form
 template <bool MIXED>
 constexpr int kGridTiles = MIXED ? 2 : 1;
+// gridding groups of the compensated mixed form (each with a high and a low
+// tile)
+constexpr int kCompGroups = 1;
+// gridding groups of a form
+template <bool MIXED, bool COMP>
+constexpr int kGroups = COMP ? kCompGroups : kGridTiles<MIXED>;
 
 template <>
 struct Form<false> {
@@ -545,6 +506,28 @@ struct GridCursor {
   int first, stride, end;
 };
 
+// a - b rounded once (an FMA with -1: the product is exact), two lanes
+__device__ __forceinline__ float2 fsub2_rn(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+
+// Compensated add of x into the tile cell (hi, lo) at shared address a,
+// with the low part lo_off bytes further: hi + x = s + err exactly (Knuth's
+// two-sum in round-to-nearest), hi <- s, lo <- lo + err.  The pair holds the
+// cell's sum to within the rounding of lo, so a tile pass of any length
+// adds no FP32 accumulation error beyond that.
+__device__ __forceinline__ void two_sum_add(uint32_t a, uint32_t lo_off,
+                                            float2 x) {
+  const float2 hi = ptx::lds_f2(a);
+  const float2 lo = ptx::lds_f2(a + lo_off);
+  const float2 sum = __fadd2_rn(hi, x);
+  const float2 bp = fsub2_rn(sum, hi);
+  const float2 err = __fadd2_rn(fsub2_rn(hi, fsub2_rn(sum, bp)),
+                                fsub2_rn(x, bp));
+  ptx::sts_f2(a, sum);
+  ptx::sts_f2(a + lo_off, __fadd2_rn(lo, err));
+}
+
 template <int N, bool MIXED>
 __device__ __forceinline__ GridCursor<N> grid_prepare(
     const VisGeom& g, const int (&pp)[N], uint32_t cfs, uint32_t gtile, int R,
@@ -564,10 +547,11 @@ __device__ __forceinline__ GridCursor<N> grid_prepare(
   return k;
 }
 
-template <int N, bool MIXED, bool DENSE, bool SCREEN>
+template <int N, bool MIXED, bool DENSE, bool SCREEN, bool COMP>
 __device__ __forceinline__ void grid_cells(const VisGeom& g, const int (&pp)[N],
                                            GridCursor<N> k,
-                                           const float2 (&gv)[N]) {
+                                           const float2 (&gv)[N],
+                                           uint32_t lo_off) {
   const int tx = g.tx, ncell = k.end, first = k.first, stride = k.stride;
   CellWalk& w = k.w;
   const uint32_t(&po)[N] = k.po;
@@ -626,15 +610,22 @@ __device__ __forceinline__ void grid_cells(const VisGeom& g, const int (&pp)[N],
           s2 = __ffma2_rn(cf, gb[v], s2);
         }
       }
-      const float2 t = ptx::lds_f2(w.tile);
-      ptx::sts_f2(w.tile, __fadd2_rn(t, make_float2(s1.x + s2.y, s1.y + s2.x)));
+      const float2 inc = make_float2(s1.x + s2.y, s1.y + s2.x);
+      if constexpr (COMP) {
+        two_sum_add(w.tile, lo_off, inc);
+      } else {
+        const float2 t = ptx::lds_f2(w.tile);
+        ptx::sts_f2(w.tile, __fadd2_rn(t, inc));
+      }
     }
     w.next(tx);
     ca += dca;
   }
 }
 
-template <int N, bool MIXED, bool DENSE>
+// COMP (mixed form only): compensated grid tiles, a low-part tile beside
+// each group's tile, updated by two-sum
+template <int N, bool MIXED, bool DENSE, bool COMP>
 __global__ void __launch_bounds__(kThreadsTiled, 1)
 tiled_kernel(const __grid_constant__ TiledParams p,
              const __grid_constant__ CUtensorMap model_map) {
@@ -670,6 +661,9 @@ tiled_kernel(const __grid_constant__ TiledParams p,
   int* req_off = ring_off + kSlots;   // ring offset of a requested copy
   int* req_pst = req_off + kSlots;    // its CF plane stride
   int* req_desc = req_pst + kSlots;   // its descriptor index
+  // last visibility whose copies were issued into slot s (-1: none), for the
+  // drain before exit
+  int* issued = req_desc + kSlots;
   TileDesc* descs = reinterpret_cast<TileDesc*>(sm + L.desc);
   unsigned char* ring = sm + L.ring;
   MT* mtile = reinterpret_cast<MT*>(sm + L.model);
@@ -687,7 +681,9 @@ tiled_kernel(const __grid_constant__ TiledParams p,
   // degridding warps' hand-off (dgfull) that followed their last read.
   // Without gridding the exchange warp releases it too (the gridding warps
   // then only wait for the copies).
-  constexpr int kGT = kGridTiles<MIXED>;
+  constexpr int kGT = kGroups<MIXED, COMP>;
+  constexpr int kTiles = kGT * (COMP ? 2 : 1);  // grid tiles in shared memory
+  static_assert(MIXED || !COMP, "compensated tiles are a mixed-form option");
   const uint32_t empty_count = uint32_t(kGR / kGT + (p.do_grid ? 0 : 1));
 
   if (tid == 0) {
@@ -703,7 +699,10 @@ tiled_kernel(const __grid_constant__ TiledParams p,
     }
     for (int x = 0; x < kSlots; ++x) ptx::mbar_init(&gvfull[x], 1);
     for (int x = 0; x < kSlots; ++x) ptx::mbar_init(&req[x], 1);
+    for (int x = 0; x < kSlots; ++x) issued[x] = -1;
     *abort = 0;
+    reinterpret_cast<ptx::WaitCtl*>(const_cast<int*>(abort))->limit_ns =
+        p.wait_limit_ns;
     ptx::fence_mbar_init();
   }
   __syncthreads();
@@ -724,6 +723,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       gpk[w] |= uint32_t(p.gpos[row][w][v] & 0xff) << (8 * v);
     }
 
+  int model_loads = 0;  // model-tile copies issued (thread 0 issues them)
   if (warp >= kPWarp) {
     // ---------------- producer warps ----------------
     // kPWarp: lane k holds the slice reference of visibility base+k of the
@@ -745,7 +745,11 @@ tiled_kernel(const __grid_constant__ TiledParams p,
     }
     const bool cf_needed = exchange || p.do_grid;
     // the copies of one visibility into slot s (one thread)
-    auto issue = [&](int s, int roff, long long off, int pstride, int dindex) {
+    auto issue = [&](int s, int roff, long long off, int pstride, int dindex,
+                     uint32_t qv) {
+      // test hook: CTA 0 never issues the copies of one visibility, so that
+      // the waits for them run out (the slot's phase never completes)
+      if (blockIdx.x == 0 && (long long)qv == p.withhold_vis) return;
       const uint32_t pbytes = uint32_t(pstride) * 8u;
       const uint32_t need = cf_needed ? uint32_t(nplanes) * pbytes : 0u;
       ring_off[s] = roff;
@@ -762,6 +766,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
                           slice + size_t(run_plane[u]) * pstride,
                           uint32_t(run_len[u]) * pbytes, &full[s]);
       }
+      issued[s] = int(qv);
     };
     uint32_t q = 0;
     if (warp != kPWarp) {
@@ -774,7 +779,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           const int s = int(qq % uint32_t(kSlots));
           ok &= ptx::mbar_wait(&req[s], (qq / kSlots) & 1, abort);
           if (lane == 0 && !*abort)
-            issue(s, req_off[s], req_src[s], req_pst[s], req_desc[s]);
+            issue(s, req_off[s], req_src[s], req_pst[s], req_desc[s], qq);
           __syncwarp();
         }
         q += uint32_t(count);
@@ -784,7 +789,6 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       unsigned long long head = 0;      // ring bytes allocated (monotonic)
       uint32_t pos = 0;                 // head modulo the ring size
       unsigned long long tail = 0;      // ring bytes released (monotonic)
-      TT_DECL(2);
       for (unsigned c = cid; c < nchunks; c += ncl) {
         const Chunk ch = p.chunks[c];
         SliceRef cur{};
@@ -802,7 +806,6 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           const uint32_t pbytes = uint32_t(pstride) * 8u;
           const uint32_t need = cf_needed ? uint32_t(nplanes) * pbytes : 0u;
           const uint32_t rb = uint32_t(p.ring_bytes);
-          TT_BEGIN();
           for (;;) {
             unsigned long long h = head;
             uint32_t ps = pos;
@@ -826,14 +829,12 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             tail = slot_end[so];
             ++q_old;
           }
-          TT_END(0);
           const int s = int(q % uint32_t(kSlots));
           // after an abort nothing is copied into slots that may still be read
           if (lane == 0 && !*abort) {
-            TT_BEGIN();
             slot_end[s] = head + need;
             if ((q & 1) == 0) {
-              issue(s, int(pos), off, pstride, ch.start + k);
+              issue(s, int(pos), off, pstride, ch.start + k, q);
             } else {
               req_off[s] = int(pos);
               req_src[s] = off;
@@ -841,14 +842,12 @@ tiled_kernel(const __grid_constant__ TiledParams p,
               req_desc[s] = ch.start + k;
               ptx::mbar_arrive(&req[s]);
             }
-            TT_END(1);
           }
           head += need;
           pos += need;
           __syncwarp();
         }
       }
-      if (lane == 0) { TT_STORE(blockIdx.x * 16 + 12, 2); }
     }
   } else {
     // ---------------- consumer roles ----------------
@@ -857,7 +856,6 @@ tiled_kernel(const __grid_constant__ TiledParams p,
     // through mbarriers; all of them meet at chunk boundaries.
     uint32_t q = 0;
     uint32_t model_phase = 0;
-    TT_DECL(10);
     // the model tile of this cluster's chunk cc, copied by one thread.  FP64
     // form: the first chunk's here, each next one's as soon as the
     // degridding warps (its only readers) are done with the current one, so
@@ -874,6 +872,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       ptx::mbar_expect_tx(model_bar, uint32_t(p.model_bytes));
       ptx::tma_load_3d(mtile, &model_map, 2 * mx, my, mc * p.nrow + row,
                        model_bar);
+      ++model_loads;
     };
     if (kEarlyModel && exchange && tid == 0 && cid < nchunks && !*abort)
       load_model(cid);
@@ -884,11 +883,10 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       const int ty = (tile / p.ntx) % p.nty;
       const int cube = tile / (p.ntx * p.nty);
       const int x0 = tx * p.T, y0 = ty * p.T;
-      TT_BEGIN();
       ptx::named_sync(1, kConsumers);
       if (!kEarlyModel && exchange && tid == 0 && !*abort) load_model(c);
       if (p.do_grid)
-        for (int i = tid; i < RR * kGT; i += kConsumers) {
+        for (int i = tid; i < RR * kTiles; i += kConsumers) {
           GT z;
           z.x = 0;
           z.y = 0;
@@ -899,7 +897,6 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         model_phase ^= 1;
       }
       ptx::named_sync(1, kConsumers);
-      TT_END(0);
       double wchunk = 0.0;
 
       if (warp < kDG) {
@@ -908,11 +905,8 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         for (int k = 0; k < ch.count; ++k, ++q) {
           const int s = int(q % uint32_t(kSlots));
           if (!exchange || int(q % kDGGroups) != grp) continue;
-          TT_BEGIN();
           ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
-          TT_END(1);
           if (ptx::warp_flag(abort)) continue;
-          TT_BEGIN();
           double acc[2 * N];
 #pragma unroll
           for (int t = 0; t < 2 * N; ++t) acc[t] = 0.0;
@@ -973,7 +967,6 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           v1 += __shfl_xor_sync(0xffffffffu, v1, 1);
           const int vidx = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 +
                            ((lane >> 2) & 1);
-          TT_END(2);
           const int b = int(q & 1);
           if (q >= 2) ok &= ptx::mbar_wait(&dgempty[b], ((q >> 1) & 1) ^ 1, abort);
           if (ptx::warp_flag(abort)) continue;
@@ -1008,16 +1001,11 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             // with degridding, the degridding warps' hand-off (dgfull)
             // follows their own wait on the slot's copies and covers it
             const int s = int(q % uint32_t(kSlots));
-            TT_BEGIN();
             if (!exchange) ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
-            TT_END(1);
             if (exchange && !ptx::warp_flag(abort)) {
               const int xs = int(q % uint32_t(kXSlots));
               const int b = xw;
-              TT_BEGIN();
               ok &= ptx::mbar_wait(&dgfull[b], (q >> 1) & 1, abort);
-              TT_END(2);
-              TT_BEGIN();
               const bool live = !ptx::warp_flag(abort);
               double tot = 0.0;
               if (live && lane < 2 * N)
@@ -1035,12 +1023,10 @@ tiled_kernel(const __grid_constant__ TiledParams p,
               if (live && r < p.nrow)
                 ptx::st_async_f64(&xbuf[((xs * 4 + row) * 4) * 2 + t],
                                   uint32_t(r), v, &xchg[xs]);
-              TT_END(4);
             }
           }
           {
             const int s = int(q % uint32_t(kSlots));
-            TT_BEGIN();
             const uint32_t qq = q;
             const TileDesc& d = descs[s];
             const int xs = int(qq % uint32_t(kXSlots));
@@ -1057,8 +1043,6 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             const double twgt = d.twgt[row];
             if (exchange)
               ok &= ptx::mbar_wait_cluster(&xchg[xs], (qq / kXSlots) & 1, abort);
-            TT_END(3);
-            TT_BEGIN();
             const bool live = !ptx::warp_flag(abort);
             float2 gout = make_float2(0.f, 0.f);
             if (live && lane < N) {
@@ -1106,7 +1090,6 @@ tiled_kernel(const __grid_constant__ TiledParams p,
                 ptx::mbar_arrive(&empty[s]);
             }
             __syncwarp();
-            TT_END(5);
           }
         }
       } else {
@@ -1122,6 +1105,9 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         const int grp = gw / gper;
         const uint32_t mytile =
             ptx::smem(gtile) + uint32_t(grp * RR) * uint32_t(sizeof(GT));
+        // compensated tiles: the low parts of the groups' tiles follow their
+        // high parts
+        const uint32_t lo_off = uint32_t(kGT * RR) * uint32_t(sizeof(GT));
         bool first = true;  // the group's first visibility of the chunk
         for (int k = 0; k < ch.count; ++k, ++q) {
           if (int(q % uint32_t(kGT)) != grp) continue;
@@ -1133,9 +1119,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             // degridding warps' hand-off that followed theirs), so this one
             // wait also covers the slot: a wait on an mbarrier whose phase
             // is already complete still costs ~100 cycles here.
-            TT_BEGIN();
             ok &= ptx::mbar_wait(&gvfull[gs], (q / kSlots) & 1, abort);
-            TT_END(1);
             // loop state from the descriptor, formed while the other
             // gridding warps may still work on the previous visibility
             const VisGeom vg = vis_geom(descs[s]);
@@ -1146,7 +1130,6 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             const GridCursor<N> cur = grid_prepare<N, MIXED>(
                 vg, pp, ptx::smem(ring) + uint32_t(ring_off[s]), mytile, R,
                 (gw % gper) * 32 + lane, gper * 32, vg.tx * vg.ty);
-            TT_BEGIN();
             if (!first) {
               if constexpr (kGT == 1)
                 ptx::named_sync(2, gper * 32);
@@ -1154,8 +1137,6 @@ tiled_kernel(const __grid_constant__ TiledParams p,
                 ptx::named_sync(2 + grp, gper * 32);
             }
             first = false;
-            TT_END(6);
-            TT_BEGIN();
             if (!ptx::warp_flag(abort)) {
               float2 gv[N];
 #pragma unroll
@@ -1164,32 +1145,29 @@ tiled_kernel(const __grid_constant__ TiledParams p,
                 if (vg.pos_w) gv[v].y = -gv[v].y;
               }
               if (vg.screen_on)
-                grid_cells<N, MIXED, DENSE, true>(vg, pp, cur, gv);
+                grid_cells<N, MIXED, DENSE, true, COMP>(vg, pp, cur, gv, lo_off);
               else
-                grid_cells<N, MIXED, DENSE, false>(vg, pp, cur, gv);
+                grid_cells<N, MIXED, DENSE, false, COMP>(vg, pp, cur, gv, lo_off);
             }
-            TT_END(7);
           } else {
             // nothing to grid: release the slot once its copies landed
-            TT_BEGIN();
             ok &= ptx::mbar_wait(&full[s], (q / kSlots) & 1, abort);
-            TT_END(1);
           }
           __syncwarp();
           if (lane == 0) ptx::mbar_arrive(&empty[s]);
         }
       }
-      TT_BEGIN();
       ptx::named_sync(1, kConsumers);
       if (p.do_grid && !*abort) {
         double2* plane = p.grid + size_t(cube * p.nrow + row) * p.ny * p.nx;
         for (int i = tid; i < RR; i += kConsumers) {
           const int gx = x0 + i % R, gy = y0 + i / R;
           if (gx < p.nx && gy < p.ny) {
-            // the gridding groups' tiles, summed in FP64
+            // the gridding groups' tiles (with their low parts), summed in
+            // FP64
             double vx = 0.0, vy = 0.0;
 #pragma unroll
-            for (int t = 0; t < kGT; ++t) {
+            for (int t = 0; t < kTiles; ++t) {
               const GT v = gtile[t * RR + i];
               vx += double(v.x);
               vy += double(v.y);
@@ -1205,19 +1183,22 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             wchunk != 0.0)
           atomicAdd(p.weights + size_t(cube) * p.nrow + row, wchunk);
       }
-      TT_END(8);
     }
-    // timer slots: degridding warp 0 -> 0..3, exchange warp -> 4..6,
-    // first gridding warp -> 7..9
-    if (lane == 0 && warp == 0) {
-      TT_PUT(0, 0); TT_PUT(1, 1); TT_PUT(2, 2); TT_PUT(3, 8);
-    }
-    if (lane == 0 && warp == kXBase) {
-      TT_PUT(4, 1); TT_PUT(5, 4); TT_PUT(6, 5); TT_PUT(10, 2); TT_PUT(11, 3);
-    }
-    if (lane == 0 && warp == kGRBase) {
-      TT_PUT(7, 1); TT_PUT(8, 6); TT_PUT(9, 7);
-    }
+  }
+  // Drain: after an abort the waits return early, so bulk copies issued
+  // into this CTA's shared memory may still be in flight; each has landed
+  // before the CTA leaves (on the normal path each was waited for already,
+  // and these waits return at once).  The exchange's st.async stores into
+  // peers are weak memory operations of their issuing threads, ordered
+  // before the release of the cluster barrier below.
+  __syncthreads();
+  if (tid == 0) {
+    for (int s = 0; s < kSlots; ++s)
+      if (issued[s] >= 0)
+        ok &= ptx::mbar_drain(&full[s], (uint32_t(issued[s]) / kSlots) & 1,
+                              abort);
+    if (model_loads > 0)
+      ok &= ptx::mbar_drain(model_bar, uint32_t(model_loads - 1) & 1, abort);
   }
   if (!ok) atomicOr(p.status, kStatusWaitTimeout);
   __syncwarp();
@@ -1336,15 +1317,18 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
   // footprints covers.  kMinRingParts is the least the plan takes.
   constexpr int kMinRingParts = 2;
   constexpr size_t kMinVisPerTile = 32;
-  const bool fixed = g->tiled_ring_parts > 0;
-  const int m_hi = fixed ? g->tiled_ring_parts : 5;
-  const int m_lo = fixed ? g->tiled_ring_parts : kMinRingParts;
+  const hpgb_tiled_plan& tp = g->tplan;
+  const bool fixed = tp.ring_parts > 0;
+  const int m_hi = fixed ? tp.ring_parts : 5;
+  const int m_lo = fixed ? tp.ring_parts : kMinRingParts;
   if (m_lo < kMinRingParts) {
     pl.why = "the CF ring must hold at least two parts";
     return pl;
   }
-  // grid tiles: one per gridding group
-  const int gt = mixed ? kGridTiles<true> : kGridTiles<false>;
+  // grid tiles: one per gridding group, and in the compensated mixed form
+  // a low-part tile beside each
+  const bool comp = mixed && do_grid && tp.compensated == HPGB_COMPENSATED_ON;
+  const int gt = comp ? 2 * kCompGroups : mixed ? kGridTiles<true> : kGridTiles<false>;
   for (int m = m_hi; m >= m_lo; --m) {
     const int rb = m * part;
     const SmemLayout L0 = smem_layout(rb, 0, em, eg, gt);
@@ -1353,6 +1337,10 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
     const int per_cell = em + eg * gt;
     int R = per_cell > 0 ? int(std::sqrt(double(left) / double(per_cell))) : 128;
     R = std::min(R, 128) & ~1;
+    if (tp.tile_side > 0) {
+      if (tp.tile_side > R) continue;  // no room for the requested side
+      R = tp.tile_side;
+    }
     if (R - taps + 1 < 4) continue;
     if (!fixed && m > m_lo) {
       const size_t T = size_t(R - taps + 1);
@@ -1369,8 +1357,9 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
     return pl;
   }
   pl.T = pl.R - taps + 1;
-  pl.K = g->tiled_chunk_vis > 0 ? g->tiled_chunk_vis
-                                : (mixed ? kChunkVisMixed : kChunkVisFP64);
+  pl.K = tp.chunk_vis > 0
+             ? tp.chunk_vis
+             : (!mixed ? kChunkVisFP64 : comp ? kChunkVisMixedComp : kChunkVisMixed);
   pl.smem = smem_layout(pl.ring_bytes, pl.R, em, eg, gt).total + 1024;
   if (em > 0 && (2 * size_t(g->grid_size[0]) * (mixed ? 4 : 8)) % 16 != 0) {
     pl.why = "model row pitch not a 16-byte multiple";
@@ -1389,6 +1378,7 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
   p.esize_model = em;
   p.esize_grid = eg;
   p.grid_tiles = gt;
+  p.compensated = comp;
   p.do_degrid = do_degrid;
   p.do_grid = do_grid;
   p.update_weights = (flags & HPGB_UPDATE_GRID_WEIGHTS) != 0;
@@ -1403,8 +1393,9 @@ Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
   using MT = typename Form<MIXED>::model_t;
   using GT = typename Form<MIXED>::grid_t;
   // the kernel places its tiles with these sizes; they must match the form
+  const bool comp = MIXED && p.compensated;
   if ((p.esize_model != 0 && p.esize_model != int(sizeof(MT))) ||
-      p.grid_tiles != kGridTiles<MIXED> ||
+      p.grid_tiles != (comp ? 2 * kCompGroups : kGridTiles<MIXED>) ||
       (p.esize_grid != 0 && p.esize_grid != int(sizeof(GT))) ||
       smem_layout(p.ring_bytes, p.R, p.esize_model, p.esize_grid,
                   p.grid_tiles).total +
@@ -1420,7 +1411,10 @@ Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
     for (int w = 0; w < 2; ++w)
       for (int v = 0; v < N; ++v)
         dense = dense && p.dpos[r][w][v] >= 0 && p.gpos[r][w][v] >= 0;
-  auto kern = dense ? tiled_kernel<N, MIXED, true> : tiled_kernel<N, MIXED, false>;
+  auto kern = dense ? (comp ? tiled_kernel<N, MIXED, true, MIXED>
+                            : tiled_kernel<N, MIXED, true, false>)
+                   : (comp ? tiled_kernel<N, MIXED, false, MIXED>
+                           : tiled_kernel<N, MIXED, false, false>);
   HPGB_CUDA_TRY(cudaFuncSetAttribute(
       kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   cudaLaunchConfig_t cfg = {};
@@ -1460,18 +1454,17 @@ Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
 }
 
 template <int N>
-Status grid_tiled_n(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
-                    const Plan& plan, bool mixed) {
+Status prepare_tiles_n(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
+                       int nty, int K, TilePrep* out) {
   VisBuffers& vb = g->vb;
   const GridGeom geom = g->geom();
   const CFGroup* groups = g->cf.desc.as<const CFGroup>();
   TileGeom tg;
-  tg.T = plan.T;
-  tg.ntx = plan.p.ntx;
-  tg.nty = plan.p.nty;
+  tg.T = T;
+  tg.ntx = ntx;
+  tg.nty = nty;
   tg.ntiles = tg.ntx * tg.nty * int(g->grid_size[3]);
   const int ntiles = tg.ntiles;
-  const int K = plan.K;
   const size_t max_chunks = n / K + size_t(ntiles) + 1;
   // scratch
   HPGB_TRY(vb.keys.reserve(n * 4));
@@ -1532,6 +1525,24 @@ Status grid_tiled_n(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
   HPGB_CUDA_TRY(cudaGetLastError());
   ++g->launches;
 
+  out->descs = descs;
+  out->srefs = srefs;
+  out->chunks = vb.items.as<Chunk>();
+  out->num_chunks = num_chunks;
+  out->max_chunks = max_chunks;
+  return Status::ok();
+}
+
+template <int N>
+Status grid_tiled_n(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
+                    const Plan& plan, bool mixed) {
+  TilePrep prep;
+  HPGB_TRY(prepare_tiles_n<N>(g, d_vis, n, plan.T, plan.p.ntx, plan.p.nty,
+                              plan.K, &prep));
+  VisBuffers& vb = g->vb;
+  TileDesc* descs = const_cast<TileDesc*>(prep.descs);
+  SliceRef* srefs = const_cast<SliceRef*>(prep.srefs);
+  unsigned* num_chunks = const_cast<unsigned*>(prep.num_chunks);
   TiledParams p = plan.p;
   p.descs = descs;
   p.srefs = srefs;
@@ -1543,15 +1554,8 @@ Status grid_tiled_n(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
   p.records = static_cast<unsigned char*>(d_vis);
   p.rec_stride = int(sizeof(VisData<N>));
   p.status = vb.counters.as<unsigned>();
-  p.timers = nullptr;
-#ifdef HPGB_TILED_TIMERS
-  {
-    static DevBuf timer_buf;
-    HPGB_TRY(timer_buf.reserve(148 * 16 * 8));
-    p.timers = timer_buf.as<unsigned long long>();
-    g_tiled_timers = p.timers;
-  }
-#endif
+  p.wait_limit_ns = g->wait_limit_ns;
+  p.withhold_vis = g->withhold_vis;
 
   CUtensorMap map;
   std::memset(&map, 0, sizeof(map));
@@ -1596,6 +1600,25 @@ Status grid_tiled_n(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
 
 }  // namespace
 
+Status prepare_tiles(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
+                     int nty, int K, TilePrep* out) {
+  switch (g->npol) {
+    case 1: return prepare_tiles_n<1>(g, d_vis, n, T, ntx, nty, K, out);
+    case 2: return prepare_tiles_n<2>(g, d_vis, n, T, ntx, nty, K, out);
+    case 3: return prepare_tiles_n<3>(g, d_vis, n, T, ntx, nty, K, out);
+    case 4: return prepare_tiles_n<4>(g, d_vis, n, T, ntx, nty, K, out);
+    default: return Status::err(HPGB_ERROR_OTHER, "bad polarization count");
+  }
+}
+
+bool tiled_plan_side(const hpgb_gridder* g, unsigned flags, size_t n,
+                     int* side) {
+  const Plan plan =
+      make_plan(g, flags, g->precision == HPGB_PRECISION_MIXED, n);
+  *side = plan.ok ? plan.R : 0;
+  return plan.ok;
+}
+
 Status grid_tiled(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
                   bool* used) {
   *used = false;
@@ -1620,14 +1643,3 @@ Status grid_tiled(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
 
 }  // namespace hpgb
 
-#ifdef HPGB_TILED_TIMERS
-// measurement builds only: copy out and clear the phase counters
-extern "C" __attribute__((visibility("default"))) int hpgb_debug_tiled_timers(
-    unsigned long long* out, int n) {
-  if (!hpgb::g_tiled_timers) return 1;
-  cudaDeviceSynchronize();
-  cudaMemcpy(out, hpgb::g_tiled_timers, size_t(n) * 8, cudaMemcpyDeviceToHost);
-  cudaMemset(hpgb::g_tiled_timers, 0, 148 * 16 * 8);
-  return 0;
-}
-#endif

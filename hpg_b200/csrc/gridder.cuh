@@ -90,9 +90,12 @@ struct hpgb_gridder {
   bool model32_valid = false;
   int kernel_kind = HPGB_KERNEL_AUTO;
   int last_kernel = HPGB_KERNEL_AUTO;  // kernel of the last non-empty batch
-  // tiled-kernel plan overrides (0: chosen by the plan)
-  int tiled_ring_parts = 0;
-  int tiled_chunk_vis = 0;
+  // tiled-kernel plan overrides (fields 0: chosen by the plan)
+  hpgb_tiled_plan tplan = {0, 0, 0, 0};
+  // bound of every device-side wait of the tiled kernel, and its test hook
+  // (a visibility whose copies CTA 0 never issues; -1: none)
+  unsigned long long wait_limit_ns = 500000000ull;
+  long long withhold_vis = -1;
 
   hpgb::CFRegion cf;
   hpgb::VisBuffers vb;
@@ -134,6 +137,11 @@ Status copy_cf(hpgb_gridder* dst, const hpgb_gridder* src);
 // grid_tiled.cu: *used is false when the tiled kernel cannot take the batch
 Status grid_tiled(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
                   bool* used);
+
+// grid_tiled.cu: the uv tile side of the plan the tiled kernel would take
+// for the batch (false when no plan fits)
+bool tiled_plan_side(const hpgb_gridder* g, unsigned flags, size_t n,
+                     int* side);
 
 // autotune.cu: times tiled plans on the batch, keeps the fastest
 Status autotune_tiled(hpgb_gridder* g, const void* vis, size_t n,

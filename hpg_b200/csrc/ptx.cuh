@@ -56,11 +56,19 @@ __device__ __forceinline__ void mbar_arrive_remote(uint64_t* bar,
 // Every lane of the calling warp waits (the warp stays converged).  After a
 // first plain test, each try_wait carries a suspend-time hint, so the warp
 // sleeps in hardware until the phase completes (or the hint runs out)
-// instead of spinning.  The wait is bounded by the global timer: after
-// kWaitLimitNs it sets the CTA-wide abort flag and returns false, and the
-// caller records the timeout instead of hanging.
+// instead of spinning.  The wait is bounded by the global timer: after the
+// CTA's wait limit it sets the CTA-wide abort flag and returns false, and
+// the caller records the timeout instead of hanging.
 constexpr uint32_t kSuspendHintNs = 20000;
-constexpr uint64_t kWaitLimitNs = 500000000ull;  // 0.5 s
+constexpr uint64_t kWaitLimitNs = 500000000ull;  // default limit: 0.5 s
+
+// The CTA's wait-control block in shared memory: the abort flag, then (8
+// bytes further) the wait limit in nanoseconds.  Waits take its address.
+struct WaitCtl {
+  int flag;
+  int pad;
+  unsigned long long limit_ns;
+};
 
 __device__ __forceinline__ uint64_t global_ns() {
   uint64_t t;
@@ -113,18 +121,24 @@ __device__ __forceinline__ bool mbar_try_cluster_suspend(uint32_t a,
   return done != 0;
 }
 
-// `abort` is a CTA-wide shared-memory flag: a wait that gives up sets it,
-// and every later wait returns false at once, so a broken pipeline ends
+__device__ __forceinline__ uint64_t wait_limit(volatile int* abort) {
+  return *reinterpret_cast<volatile unsigned long long*>(
+      reinterpret_cast<volatile char*>(abort) + 8);
+}
+
+// `abort` is the flag of the CTA's WaitCtl block: a wait that gives up sets
+// it, and every later wait returns false at once, so a broken pipeline ends
 // quickly with an error status instead of timing out wait after wait.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
                                           volatile int* abort) {
   const uint32_t a = smem(bar);
   if (mbar_try(a, parity)) return true;
   const uint64_t t0 = global_ns();
+  const uint64_t limit = wait_limit(abort);
   for (;;) {
     if (mbar_try_suspend(a, parity)) return true;
     if (*abort) return false;
-    if (global_ns() - t0 > kWaitLimitNs) break;
+    if (global_ns() - t0 > limit) break;
   }
   *abort = 1;
   return false;
@@ -137,13 +151,30 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar,
   const uint32_t a = smem(bar);
   if (mbar_try_cluster(a, parity)) return true;
   const uint64_t t0 = global_ns();
+  const uint64_t limit = wait_limit(abort);
   for (;;) {
     if (mbar_try_cluster_suspend(a, parity)) return true;
     if (*abort) return false;
-    if (global_ns() - t0 > kWaitLimitNs) break;
+    if (global_ns() - t0 > limit) break;
   }
   *abort = 1;
   return false;
+}
+
+// Wait for a phase whose transfer was issued (a bulk copy into this CTA's
+// shared memory), ignoring the abort flag: used before the CTA exits so
+// that no copy still lands in memory the CTA no longer owns.  Bounded by the
+// wait limit; returns false if it ran out.
+__device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity,
+                                           volatile int* abort) {
+  const uint32_t a = smem(bar);
+  if (mbar_try(a, parity)) return true;
+  const uint64_t t0 = global_ns();
+  const uint64_t limit = wait_limit(abort);
+  for (;;) {
+    if (mbar_try_suspend(a, parity)) return true;
+    if (global_ns() - t0 > limit) return false;
+  }
 }
 
 // warp-uniform read of a shared-memory flag (lane 0's view)

@@ -340,11 +340,22 @@ class Gridder:
     def shift_model(self, direction=abi.SHIFT_FORWARD):
         check(load().hpgb_shift_model(self._h, int(direction)))
 
-    def set_tiled_plan(self, ring_parts=0, chunk_vis=0):
-        """Override the tiled kernel's ring depth (in largest CF parts) and
-        visibilities per tile pass; 0 keeps the automatic choice."""
-        check(load().hpgb_set_tiled_plan(self._h, int(ring_parts),
-                                         int(chunk_vis)))
+    def set_tiled_plan(self, ring_parts=0, chunk_vis=0, tile_side=0,
+                       compensated=0):
+        """Override the tiled kernel's plan: ring depth (in largest CF
+        parts), visibilities per tile pass, uv tile side (cells) and, in the
+        mixed form, compensated tiles (abi.COMPENSATED_ON / _OFF); 0 keeps
+        the automatic choice."""
+        plan = abi.TiledPlan(int(ring_parts), int(chunk_vis), int(tile_side),
+                             int(compensated))
+        check(load().hpgb_set_tiled_plan_ex(self._h, ctypes.byref(plan)))
+
+    def tiled_plan(self):
+        """The plan overrides in force: dict of ring_parts, chunk_vis,
+        tile_side, compensated (0 = automatic)."""
+        plan = abi.TiledPlan()
+        check(load().hpgb_get_tiled_plan(self._h, ctypes.byref(plan)))
+        return {f: getattr(plan, f) for f, _ in abi.TiledPlan._fields_}
 
     def autotune_tiled(self, visibilities, flags=None, on_device=False):
         """Time the tiled kernel's candidate plans on this batch (grid and
@@ -385,6 +396,16 @@ class Gridder:
         check(load().hpgb_tiled_kernel_time(self._h, ctypes.byref(ms),
                                             ctypes.byref(n)))
         return ms.value, n.value
+
+    def set_wait_limit(self, seconds):
+        """Bound of every device-side wait of the tiled kernel (seconds)."""
+        check(load().hpgb_set_wait_limit(self._h, float(seconds)))
+
+    def debug_withhold_copy(self, visibility):
+        """Test hook: the first CTA of later tiled launches never issues the
+        copies of the visibility at this position of its sequence (-1:
+        none), so that the kernel takes its wait-timeout path."""
+        check(load().hpgb_debug_withhold_copy(self._h, int(visibility)))
 
     def last_gridding_kernel(self):
         """abi.KERNEL_TILED or abi.KERNEL_DIRECT: the kernel that took the

@@ -139,6 +139,13 @@ typedef struct hpgb_vis_coords {
   int32_t cf_size[2];     /* support (taps) */
   int32_t pos_w;          /* uvw[2] > 0 */
   int32_t in_grid;        /* all_within_grid() (src/hpg_core.hpp:1070-1080) */
+  /* Mueller routing of this visibility, [grid row][visibility pol], -1
+   * inactive: the CF Mueller plane its gridding products use
+   * ((pos_w ? mueller : conjugate)[r][v], src/hpg_core.hpp:808-817) and the
+   * plane its degridding products use ((pos_w ? conjugate : mueller)[r][v],
+   * :598-600) */
+  int32_t grid_mueller[4][4];
+  int32_t degrid_mueller[4][4];
 } hpgb_vis_coords;
 
 typedef struct hpgb_gridder hpgb_gridder;
@@ -362,6 +369,48 @@ HPGB_API int hpgb_kernel_launches(const hpgb_gridder* gridder,
 HPGB_API int hpgb_set_tiled_plan(hpgb_gridder* gridder, int ring_parts,
                                  int chunk_vis);
 
+/* The tiled kernel's whole plan, no counterpart in the reference (tuning).
+ * Every field 0 means "the plan's own choice":
+ *  ring_parts     2..16: CF ring depth, in largest per-row CF parts;
+ *  chunk_vis      1..2^20: visibilities per tile pass (between flushes of
+ *                 the shared-memory grid tile to the grid);
+ *  tile_side      even, at most 128: side R of the shared-memory uv tile in
+ *                 cells (the largest that fits the ring's leftover shared
+ *                 memory when 0); a side the ring leaves no room for makes
+ *                 the plan not fit;
+ *  compensated    mixed form only: 1: plain FP32 grid tiles; 2: FP32
+ *                 high/low tile pairs updated by two-sum, so that the tile
+ *                 adds no accumulation error however long the pass (the
+ *                 pairs take twice the tile memory: smaller tiles).
+ * hpgb_set_tiled_plan(g, r, c) sets the first two fields and clears the
+ * others. */
+typedef struct hpgb_tiled_plan {
+  int ring_parts;
+  int chunk_vis;
+  int tile_side;
+  int compensated;
+} hpgb_tiled_plan;
+enum hpgb_plan_choice { HPGB_PLAN_AUTO = 0 };
+enum hpgb_compensation { HPGB_COMPENSATED_OFF = 1, HPGB_COMPENSATED_ON = 2 };
+HPGB_API int hpgb_set_tiled_plan_ex(hpgb_gridder* gridder,
+                                    const hpgb_tiled_plan* plan);
+HPGB_API int hpgb_get_tiled_plan(const hpgb_gridder* gridder,
+                                 hpgb_tiled_plan* plan);
+
+/* Bound of every device-side wait of the tiled kernel, in seconds (0.5 by
+ * default; 1e-4..60), no counterpart in the reference.  A wait that runs out
+ * ends the launch early with an error status: the next hpgb_fence returns
+ * HPGB_ERROR_OTHER ("a device-side wait gave up"), the batch's results are
+ * incomplete, and the gridder stays usable. */
+HPGB_API int hpgb_set_wait_limit(hpgb_gridder* gridder, double seconds);
+
+/* Test hook, no counterpart in the reference: the first CTA of the next
+ * tiled launches never issues the bulk copies of the visibility at this
+ * position of its sequence (-1: none), so that the waits for them run out
+ * and the kernel takes its timeout path.  For tests of that path only. */
+HPGB_API int hpgb_debug_withhold_copy(hpgb_gridder* gridder,
+                                      long long visibility);
+
 /* Which kernel gridded/degridded the gridder's last non-empty batch:
  * HPGB_KERNEL_TILED or HPGB_KERNEL_DIRECT (HPGB_KERNEL_AUTO before the first
  * batch).  No counterpart in the reference: it makes the tiled kernel's
@@ -370,13 +419,19 @@ HPGB_API int hpgb_last_gridding_kernel(const hpgb_gridder* gridder,
                                        int* kind);
 
 /* Autotuner of the tiled kernel, no counterpart in the reference: runs the
- * batch (as hpgb_grid_visibilities would with these flags) once per
- * candidate plan -- CF ring depths 4..8, then tile-pass lengths around the
- * fastest depth -- timing each with CUDA events, restores the grid and
- * weights after every trial, and keeps the fastest plan for the gridder's
- * later calls (as hpgb_set_tiled_plan would), returning it.  Synchronous.
- * Costs about eight runs of the batch: tune on a representative batch once,
- * then grid. */
+ * batch (as hpgb_grid_visibilities would with these flags) three times per
+ * candidate plan -- CF ring depths 2..8, then uv tile sides 8 and 16 cells
+ * below the largest that fits at the fastest depth, then tile-pass lengths
+ * -- ranks the candidates by their median CUDA-event time (a launch that
+ * reported a device wait timeout does not count), restores the grid and
+ * weights on every exit path, and keeps the fastest plan for the gridder's
+ * later calls (readable with hpgb_get_tiled_plan), returning its ring depth
+ * and pass length.  The mixed form's compensation setting is kept.  Results
+ * are cached in the process per workload (grid shape, polarizations,
+ * Mueller tables, CF group shapes, precision, compensation, flags, model,
+ * log2 of the batch size): a later call with the same workload applies the
+ * cached plan at once.  Synchronous; costs about forty runs of the batch
+ * the first time: tune on a representative batch once, then grid. */
 HPGB_API int hpgb_autotune_tiled(hpgb_gridder* gridder, const void* visibilities,
                                  size_t num_visibilities,
                                  unsigned num_polarizations, unsigned flags,

@@ -133,6 +133,8 @@ struct oracle_coords {
   int32_t cf_size[2];
   int32_t pos_w;
   int32_t in_grid;
+  int32_t grid_mueller[4][4];    // Mueller plane of the gridding products
+  int32_t degrid_mueller[4][4];  // and of the degridding products
 };
 
 }  // extern "C"
@@ -478,6 +480,13 @@ void coords(const oracle_params& p, const VisData<N>* vis, size_t n,
     }
     o.pos_w = v.pos_w;
     o.in_grid = all_within_grid(v, p.grid_size);
+    // Mueller routing: src/hpg_core.hpp:808-817 (gridding), :598-600
+    // (degridding)
+    for (int r = 0; r < 4; ++r)
+      for (int c = 0; c < 4; ++c) {
+        o.grid_mueller[r][c] = (v.pos_w ? p.mueller : p.conj_mueller)[r][c];
+        o.degrid_mueller[r][c] = (v.pos_w ? p.conj_mueller : p.mueller)[r][c];
+      }
   }
 }
 

@@ -55,7 +55,8 @@ class _Params(ctypes.Structure):
 COORDS_DTYPE = np.dtype([
     ("grid_coord", np.int32, (2,)), ("cf_major", np.int32, (2,)),
     ("cf_minor", np.int32, (2,)), ("fine_offset", np.int32, (2,)),
-    ("cf_size", np.int32, (2,)), ("pos_w", np.int32), ("in_grid", np.int32)])
+    ("cf_size", np.int32, (2,)), ("pos_w", np.int32), ("in_grid", np.int32),
+    ("grid_mueller", np.int32, (4, 4)), ("degrid_mueller", np.int32, (4, 4))])
 
 _lib = None
 

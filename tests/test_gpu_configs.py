@@ -80,7 +80,8 @@ def test_single_pol_config(gpu, oracle_lib, kernel, precision):
 FULL_POL_NVIS = 40_000
 # the plans the benchmark's autotuner chose for 10M visibilities of this
 # workload (ring parts, visibilities per tile pass)
-BENCH_PLANS = {abi.PRECISION_MIXED: (5, 512), abi.PRECISION_FP64: (5, 4096)}
+BENCH_PLANS = {abi.PRECISION_MIXED: (5, 512), abi.PRECISION_FP64: (5, 4096),
+               "mixed-comp": (5, 2048)}
 
 
 @pytest.fixture(scope="module")
@@ -146,22 +147,62 @@ def _check_full_pol(case, oracle_lib, g, precision, res):
 
 
 @pytest.mark.parametrize("plan", ["default", "bench", "autotuned"])
-@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED],
-                         ids=["fp64", "mixed"])
-def test_full_pol_config_tiled(gpu, oracle_lib, full_pol, precision, plan):
+@pytest.mark.parametrize("precision,comp",
+                         [(abi.PRECISION_FP64, 0), (abi.PRECISION_MIXED, 0),
+                          (abi.PRECISION_MIXED, abi.COMPENSATED_ON)],
+                         ids=["fp64", "mixed", "mixed-comp"])
+def test_full_pol_config_tiled(gpu, oracle_lib, full_pol, precision, comp,
+                               plan):
     """degrid_grid_get_residual_visibilities at the full-polarization
     benchmark's shapes through the tiled kernel."""
     case = full_pol
     g = _full_pol_gridder(case, "tiled", precision)
+    g.set_tiled_plan(compensated=comp)
     if plan == "bench":
-        g.set_tiled_plan(*BENCH_PLANS[precision])
+        ring, chunk = BENCH_PLANS[precision]
+        if comp:
+            ring, chunk = BENCH_PLANS["mixed-comp"]
+        g.set_tiled_plan(ring, chunk, compensated=comp)
     elif plan == "autotuned":
         ring, chunk = g.autotune_tiled(case["vis"])
-        assert 4 <= ring <= 8
+        assert 2 <= ring <= 8
+        assert g.tiled_plan()["compensated"] == comp
     fut = g.degrid_grid_get_residual_visibilities(case["vis"])
     g.fence()
     _check_full_pol(case, oracle_lib, g, precision, fut.get())
     g.close()
+
+
+def test_compensated_tiles_error(gpu, oracle_lib, full_pol):
+    """Compensated (two-sum) FP32 tiles against plain FP32 tiles at long
+    tile passes (8192 visibilities): each mixed-form grid is compared with
+    the oracle's gridding of that run's own residuals, which removes the
+    degridding error and leaves the gridding products and the tile
+    accumulation.  The compensated tiles accumulate without FP32 error, so
+    their grid error is at most half the plain tiles' and within 1e-7."""
+    O = oracle_lib
+    case = full_pol
+    p = case["p"]
+    # visibilities packed into a disk of 20 cells around the grid centre:
+    # thousands share each uv tile, so a tile pass sums thousands of them
+    vis = workloads.visibilities(30_000, 4, case["grid_size"],
+                                 p["grid_scale"], p["freq"],
+                                 np.random.default_rng(77), disk=0.01,
+                                 w_frac=0.3, ngroups=len(p["supports"]))
+    errs = {}
+    for comp in (abi.COMPENSATED_OFF, abi.COMPENSATED_ON):
+        g = _full_pol_gridder(case, "tiled", abi.PRECISION_MIXED)
+        g.set_tiled_plan(5, 8192, compensated=comp)
+        fut = g.degrid_grid_get_residual_visibilities(vis)
+        g.fence()
+        o = O.Oracle(case["grid_size"], p["grid_scale"], p["mueller"],
+                     p["conj_mueller"], p["oversampling"], case["ext"],
+                     case["hvals"])
+        o.grid_visibilities(fut.get(), nthreads=O.num_threads())
+        errs[comp] = rel_norm(g.grid_values(), o.grid)
+        g.close()
+    assert errs[abi.COMPENSATED_ON] <= 1e-7
+    assert errs[abi.COMPENSATED_ON] <= 0.5 * errs[abi.COMPENSATED_OFF]
 
 
 def test_full_pol_config_direct(gpu, oracle_lib, full_pol):

@@ -86,12 +86,23 @@ def test_coords_bit_exact(gpu, oracle_lib):
     vis["uvw"][:k, 0] = cells[:, 0] / (cfg["grid_scale"][0] * inv_lambda)
     vis["uvw"][:k, 1] = cells[:, 1] / (cfg["grid_scale"][1] * inv_lambda)
     vis["uvw"][k:2 * k, 0] = rng.uniform(-3000, 3000, k)  # partly off grid
+    # conjugate Mueller indexes transposed: the routing differs by sign of w
+    cfg["conj_mueller"] = [[c * 4 + r for c in range(4)] for r in range(4)]
     g, o = make_pair(cfg, oracle_lib)
     dc = g.debug_coords(vis)
     oc = o.vis_coords(vis)
     for name in oc.dtype.names:
         assert np.array_equal(dc[name], oc[name]), name
     assert (oc["in_grid"] == 0).any() and (oc["in_grid"] == 1).any()
+    # Mueller routing: gridding uses the Mueller indexes for w > 0 and the
+    # conjugate ones otherwise; degridding the reverse
+    pos = dc["pos_w"] == 1
+    assert pos.any() and (~pos).any()
+    mi, ci = np.array(cfg["mueller"]), np.array(cfg["conj_mueller"])
+    assert (dc["grid_mueller"][pos] == mi).all()
+    assert (dc["grid_mueller"][~pos] == ci).all()
+    assert (dc["degrid_mueller"][pos] == ci).all()
+    assert (dc["degrid_mueller"][~pos] == mi).all()
 
 
 def test_gridone_golden(gpu, oracle_lib):
@@ -214,17 +225,25 @@ def test_degrid_grid_parity(gpu, oracle_lib, grad, kernel, precision):
     np.testing.assert_allclose(g.grid_weights(), o.weights, rtol=1e-12)
 
 
-@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED],
-                         ids=["fp64", "mixed"])
-@pytest.mark.parametrize("ring_parts,chunk", [(4, 64), (6, 0), (5, 7), (4, 1),
-                                             (5, 2), (3, 0), (2, 5)])
-def test_tiled_plan_overrides(gpu, oracle_lib, precision, ring_parts, chunk):
-    """Every ring depth and tile-pass length the plan accepts gives the same
-    results: small chunks cross many tile flushes, a deep ring keeps many
-    visibilities in flight."""
+@pytest.mark.parametrize("precision,comp",
+                         [(abi.PRECISION_FP64, 0), (abi.PRECISION_MIXED, 0),
+                          (abi.PRECISION_MIXED, abi.COMPENSATED_ON)],
+                         ids=["fp64", "mixed", "mixed-comp"])
+@pytest.mark.parametrize("ring_parts,chunk,side",
+                         [(4, 64, 0), (6, 0, 0), (5, 7, 0), (4, 1, 0),
+                          (5, 2, 0), (3, 0, 0), (2, 5, 0), (4, 0, 20),
+                          (5, 3000, 16)])
+def test_tiled_plan_overrides(gpu, oracle_lib, precision, comp, ring_parts,
+                              chunk, side):
+    """Every ring depth, tile side and tile-pass length the plan accepts,
+    with and without compensated tiles, gives the same results: small
+    chunks cross many tile flushes, a deep ring keeps many visibilities in
+    flight, a small side multiplies the tiles."""
     cfg = small_full_pol(3000, grad=0.4)
     g, o = make_pair(cfg, oracle_lib, precision=precision, kernel="tiled")
-    g.set_tiled_plan(ring_parts, chunk)
+    g.set_tiled_plan(ring_parts, chunk, side, comp)
+    assert g.tiled_plan() == dict(ring_parts=ring_parts, chunk_vis=chunk,
+                                  tile_side=side, compensated=comp)
     fut = g.degrid_grid_get_residual_visibilities(cfg["vis"])
     g.fence()
     exp = o.grid_visibilities(cfg["vis"], do_degrid=True, return_vis=True)
@@ -252,7 +271,11 @@ def test_autotune_keeps_data_and_parity(gpu, oracle_lib, precision):
     g.fence()
     before = (g.grid_values(), g.grid_weights())
     ring, chunk = g.autotune_tiled(cfg["vis"])
-    assert 4 <= ring <= 8 and chunk >= 0
+    assert 2 <= ring <= 8 and chunk >= 0
+    plan = g.tiled_plan()
+    assert plan["ring_parts"] == ring and plan["chunk_vis"] == chunk
+    # the same workload again: the cached plan, at once
+    assert g.autotune_tiled(cfg["vis"]) == (ring, chunk)
     assert np.array_equal(g.grid_values(), before[0])
     assert np.array_equal(g.grid_weights(), before[1])
     rest = cfg["vis"][1000:]
@@ -299,7 +322,8 @@ def test_tiled_plan_rejects_bad_overrides(gpu, oracle_lib):
     """Ring depths outside 2..16 and negative pass lengths are refused."""
     cfg = small_full_pol(10)
     g, _ = make_pair(cfg, oracle_lib, kernel="tiled")
-    for bad in ((1, 0), (-1, 0), (17, 0), (0, -1)):
+    for bad in ((1, 0), (-1, 0), (17, 0), (0, -1), (0, 0, 129),
+                (0, 0, 33), (0, 0, -2), (0, 0, 0, 3)):
         with pytest.raises(HpgError):
             g.set_tiled_plan(*bad)
     g.set_tiled_plan(0, 0)
