@@ -47,9 +47,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--precision", default="both",
-                   choices=["both", "mixed", "fp64"],
-                   help="both: the mixed form is the headline, the FP64 form "
-                        "is timed beside it")
+                   choices=["both", "mixed", "mixed-comp", "fp64"],
+                   help="both: the mixed form is the headline, the "
+                        "compensated mixed form and the FP64 form are timed "
+                        "beside it")
     p.add_argument("--nvis", type=int, default=10_000_000)
     p.add_argument("--grid", type=int, default=2048)
     p.add_argument("--oversampling", type=int, default=128,
@@ -61,6 +62,15 @@ def parse():
                    help="skip the (untimed) autotuning of the tiled plan")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="full-pol",
+                   choices=["full-pol", "adjoint", "batch"],
+                   help="full-pol: the headline degrid+grid step; adjoint: "
+                        "one gradient step of the differentiable-imaging "
+                        "workload (D then D^H on a 4096^2 x 2 grid, 32 CF "
+                        "groups of supports 8..64, FP64 operators); batch: "
+                        "64 uneven gridding jobs, one launch per "
+                        "polarization class, against one launch per job")
+    p.add_argument("--jobs", type=int, default=64)
     return p.parse_args()
 
 
@@ -162,7 +172,7 @@ TRAFFIC_PER_VIS_FP64 = (16.291e9 - 0.805e9) / 200_000
 
 
 def kernel_traffic(form, nvis, grid_elems):
-    if form == "mixed":
+    if form.startswith("mixed"):
         return TRAFFIC_PER_VIS_MIXED * nvis + grid_elems * (8 + 32)
     return TRAFFIC_PER_VIS_FP64 * nvis + grid_elems * (16 + 32)
 
@@ -289,7 +299,7 @@ def run_reference(args, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": config_of(args, args.gpus, "mixed"
-                            if args.precision in ("both", "mixed") else "fp64"),
+                            if args.precision == "both" else args.precision),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads,
                          "kind": "port",
                          "sample": f"{n_step} visibilities per step of the "
@@ -300,6 +310,247 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+ADJ_SUPPORTS = tuple(8 + (56 * k) // 31 for k in range(32))  # 8 .. 64
+
+
+def run_adjoint(args):
+    """Gradient step of L = sum w |D(G) - V|^2 on one GPU: y = D(G) (FP64
+    degridding), r = w (y - V), dL/dG = 2 D^H(r), through the tiled
+    operators (hpgb_degrid_linear / hpgb_degrid_adjoint).  Workload: a
+    4096 x 4096 x 2 grid (diagonal Mueller), 32 w-plane CF groups of
+    supports 8..64 at oversampling 128, args.nvis visibilities (seeded
+    synthetic data of those shapes; G = point sources plus N(0, 0.01)
+    noise).  Prints one JSON line: Mvis/s of the step, each operator's
+    time and its HBM roofline (CF slice bytes per visibility, grid bytes per
+    pass)."""
+    import ctypes
+    import torch
+    import hpg_b200
+    from hpg_b200 import CFArray, Gridder, abi, workloads
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    hpg_b200.load()
+    side = 4096
+    npol = 2
+    rng = np.random.default_rng(20261207)
+    supports = ADJ_SUPPORTS
+    os_ = args.oversampling
+    mf = np.ones(npol, np.complex128)
+    w_phases = [0.01 * k for k in range(len(supports))]
+    ext, vals = workloads.separable_cf_torch(supports, os_, mf, dev,
+                                             w_phases=w_phases)
+    gs = (side, side, npol, 1)
+    scale = (0.0476591, 0.0476591)
+    vis = workloads.visibilities(args.nvis, npol, gs, scale, 1.4e9, rng,
+                                 w_frac=0.3, ngroups=len(supports))
+    mi = [[0, -1], [-1, 1]]
+    g = Gridder.create(0, 0, args.nvis, None, gs, scale, mi, mi)
+    g.set_convolution_function(CFArray(os_, ext, vals), on_device=True)
+    del vals
+    torch.cuda.empty_cache()
+    dvis = torch.from_numpy(vis.view(np.uint8)).to(dev)
+    gen = torch.Generator(device=dev).manual_seed(11)
+    G = (torch.randn((1, npol, side, side), generator=gen, device=dev,
+                     dtype=torch.float64) * 0.01 + 0j)
+    pts = torch.randint(0, side, (1000, 2), generator=gen, device=dev)
+    G[0, :, pts[:, 1], pts[:, 0]] += 1.0
+    V = torch.from_numpy(vis["vis"].astype(np.complex128)).to(dev)
+    W = torch.from_numpy(vis["weights"].astype(np.float64)).to(dev)
+    y = torch.empty((args.nvis, npol), dtype=torch.complex128, device=dev)
+    grad = torch.zeros_like(G)
+    lib = abi.load()
+    stream = torch.cuda.ExternalStream(g.stream, device=dev)
+    P = ctypes.c_void_p
+
+    def step(ev=None):
+        abi.check(lib.hpgb_degrid_linear(g._h, P(dvis.data_ptr()), args.nvis,
+                                         npol, P(G.data_ptr()),
+                                         P(y.data_ptr())))
+        if ev:
+            ev[1].record(stream)
+        with torch.cuda.stream(stream):
+            r = (y - V) * (2.0 * W)
+            grad.zero_()
+            if ev:
+                ev[2].record(stream)
+            abi.check(lib.hpgb_degrid_adjoint(g._h, P(dvis.data_ptr()),
+                                              args.nvis, npol,
+                                              P(r.data_ptr()),
+                                              P(grad.data_ptr())))
+        return r
+
+    for _ in range(args.warmup):
+        step()
+    g.fence()
+    torch.cuda.synchronize()
+    t_d, t_dh, t_step = [], [], []
+    for _ in range(args.steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(stream)
+        r = step(ev)
+        ev[3].record(stream)
+        ev[3].synchronize()
+        t_d.append(ev[0].elapsed_time(ev[1]))
+        t_dh.append(ev[2].elapsed_time(ev[3]))
+        t_step.append(ev[0].elapsed_time(ev[3]))
+        del r
+    assert g.last_gridding_kernel() == abi.KERNEL_TILED
+    peak, peak_kind = peaks()
+    taps = np.asarray(taps_of(supports), np.int64)[
+        vis["cf_index"][:, 1].astype(np.int64)]
+    cf_bytes = int((taps * taps).sum()) * 1 * 8 * npol  # one plane per row
+    grid_bytes = side * side * npol * 16
+    vals_bytes = args.nvis * npol * 16
+    # algorithmic bytes per operator launch: the CF slices once, the grid
+    # once (D reads the model; D^H reads and writes the gradient), the
+    # visibility values once
+    b_d = cf_bytes + grid_bytes + vals_bytes
+    b_dh = cf_bytes + 2 * grid_bytes + vals_bytes
+    ms_d, ms_dh = statistics.median(t_d), statistics.median(t_dh)
+    ms_step = statistics.median(t_step)
+    line = {
+        "metric": "Mvis/s loss-gradient step (D then D^H), 4096^2x2, "
+                  "supports 8-64",
+        "value": args.nvis / (ms_step * 1e-3) / 1e6, "unit": "Mvis/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"differentiable degridding 4096x4096x2, 32 "
+                               f"CF groups (supports 8-64, os {os_}), "
+                               f"diagonal Mueller",
+                   "nvis": args.nvis},
+        "operators": {
+            "D": {"ms": ms_d, "gbs": b_d / (ms_d * 1e-3) / 1e9,
+                  "frac": b_d / (ms_d * 1e-3) / 1e9 / peak,
+                  "algorithmic_bytes": b_d},
+            "D^H": {"ms": ms_dh, "gbs": b_dh / (ms_dh * 1e-3) / 1e9,
+                    "frac": b_dh / (ms_dh * 1e-3) / 1e9 / peak,
+                    "algorithmic_bytes": b_dh},
+        },
+        "cf_bytes_per_vis": cf_bytes / args.nvis,
+        "peak": peak, "peak_kind": peak_kind,
+    }
+    print(json.dumps(line), flush=True)
+    g.close()
+
+
+def run_batch(args):
+    """The batched, uneven workload: args.jobs independent gridding jobs,
+    each with a grid side log-uniform in [256, 2048], 1, 2 or 4
+    polarizations (diagonal Mueller), a batch log-uniform in [10k, 2M]
+    visibilities (uv uniform in the disk), 1..16 CF groups with supports
+    drawn from {8, 16, 32, 64} at oversampling 64; mixed form.  One step
+    grids every job's batch: the jobs of each polarization class go to one
+    hpgb_grid_visibilities_batch call (one persistent tiled launch per
+    class, three at most), device-resident inputs.  The same step is timed
+    with one call per job (one tiled launch each) beside it.  Prints one JSON line: Mvis/s of both, and the
+    batched launches' HBM roofline (records + CF slices once per visibility
+    + grid read/write per job)."""
+    import torch
+    import hpg_b200
+    from hpg_b200 import CFArray, Gridder, abi, workloads
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    hpg_b200.load()
+    rng = np.random.default_rng(20261206)
+    os_ = 64
+    scale = (0.0476591, 0.0476591)
+    jobs = []
+    for j in range(args.jobs):
+        side = int(np.exp(rng.uniform(np.log(256), np.log(2048)))) & ~1
+        npol = int(rng.choice([1, 2, 4]))
+        nvis = int(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        ngroups = int(rng.integers(1, 17))
+        supports = [int(x) for x in rng.choice([8, 16, 32, 64], ngroups)]
+        mi = [[r if c == r else -1 for c in range(npol)] for r in range(npol)]
+        gs = (side, side, npol, 1)
+        ext, vals = workloads.separable_cf_torch(
+            supports, os_, np.ones(npol) + 0.1j * rng.standard_normal(npol),
+            dev)
+        g = Gridder.create(0, 0, nvis, None, gs, scale, mi, mi)
+        g.set_precision(abi.PRECISION_MIXED)
+        g.set_convolution_function(CFArray(os_, ext, vals), on_device=True)
+        del vals
+        vis = workloads.visibilities(nvis, npol, gs, scale, 1.4e9, rng,
+                                     ngroups=ngroups)
+        dvis = torch.from_numpy(vis.view(np.uint8)).to(dev)
+        taps = np.asarray(taps_of(supports), np.int64)[
+            vis["cf_index"][:, 1].astype(np.int64)]
+        jobs.append(dict(g=g, dvis=dvis, npol=npol, nvis=nvis, side=side,
+                         bytes=int(len(vis) * vis.dtype.itemsize +
+                                   (taps * taps).sum() * npol * 8 +
+                                   2 * side * side * npol * 16)))
+        del vis
+    torch.cuda.empty_cache()
+    classes = {}
+    for job in jobs:
+        classes.setdefault(job["npol"], []).append(job)
+    total_vis = sum(j["nvis"] for j in jobs)
+    total_bytes = sum(j["bytes"] for j in jobs)
+    def batched():
+        for cls in classes.values():
+            hpg_b200.grid_visibilities_batch(
+                [j["g"] for j in cls], [j["dvis"] for j in cls],
+                on_device=True)
+
+    def per_job():
+        for job in jobs:
+            job["g"].grid_visibilities(job["dvis"], on_device=True)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        for job in jobs:
+            job["g"].fence()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(args.steps):
+            fn()
+        for job in jobs:  # every gridder's work before the end event
+            e = torch.cuda.Event()
+            e.record(torch.cuda.ExternalStream(job["g"].stream, device=dev))
+            torch.cuda.current_stream().wait_event(e)
+        ev1.record()
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) / args.steps
+
+    # each class's launch runs on the stream of its first gridder, so the
+    # classes may overlap; the step ends when every gridder's work has
+    ms_batched = timed(batched)
+    for job in jobs:
+        job["g"].set_gridding_kernel(abi.KERNEL_TILED)
+    ms_single = timed(per_job)
+    launches = {k: len(v) for k, v in classes.items()}
+    peak, peak_kind = peaks()
+    line = {
+        "metric": "Mvis/s gridding of 64 uneven jobs (batched launches)",
+        "value": total_vis / (ms_batched * 1e-3) / 1e6, "unit": "Mvis/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_batched, "higher_is_better": True,
+        "dtype": "f32-mixed", "data": "synthetic",
+        "config": {"workload": f"{args.jobs} gridding jobs: side 256-2048 "
+                               f"log-uniform, 1/2/4 pol diagonal, 10k-2M "
+                               f"vis, 1-16 CF groups of supports "
+                               f"{{8,16,32,64}}, os {os_}",
+                   "total_vis": total_vis,
+                   "jobs_per_polarization_class": launches},
+        "per_job_launches": {"value": total_vis / (ms_single * 1e-3) / 1e6,
+                             "ms_per_step": ms_single},
+        "roofline": {"bound": "hbm", "achieved": total_bytes /
+                     (ms_batched * 1e-3) / 1e9, "peak": peak,
+                     "unit": "GB/s",
+                     "frac": total_bytes / (ms_batched * 1e-3) / 1e9 / peak,
+                     "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_step": total_bytes,
+                     "scope": "whole step (sort, descriptors, tiled launch)"},
+    }
+    print(json.dumps(line), flush=True)
+    for job in jobs:
+        job["g"].close()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -307,6 +558,12 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args)
+        return
+    if args.workload == "batch":
+        run_batch(args)
         return
     import torch
     import torch.distributed as dist
@@ -407,16 +664,29 @@ def main():
     peak, peak_kind = peaks()
     total_vis = args.nvis * world
 
-    forms = (["mixed", "fp64"] if args.precision == "both"
+    forms = (["mixed", "mixed-comp", "fp64"] if args.precision == "both"
              else [args.precision])
     results = {}
     plans = {}
     clock_summary = None
+
+    def use_form(form, plan=None):
+        """Arithmetic form: "mixed" (FP32 products and tiles), "mixed-comp"
+        (the same with compensated two-sum tile pairs) or "fp64"."""
+        g.set_precision(hpg_b200.PRECISION_FP64 if form == "fp64"
+                        else hpg_b200.PRECISION_MIXED)
+        comp = abi.COMPENSATED_ON if form == "mixed-comp" else 0
+        plan = plan or {}
+        g.set_tiled_plan(plan.get("ring_parts", 0), plan.get("chunk_vis", 0),
+                         plan.get("tile_side", 0), comp)
+
     for form in forms:
-        g.set_precision(hpg_b200.PRECISION_MIXED if form == "mixed"
-                        else hpg_b200.PRECISION_FP64)
+        use_form(form)
         # untimed set-up: the autotuner picks the tiled plan on this batch
-        plan = g.autotune_tiled(dvis, on_device=True) if args.autotune else None
+        plan = None
+        if args.autotune:
+            g.autotune_tiled(dvis, on_device=True)
+            plan = g.tiled_plan()
         plans[form] = plan
         for _ in range(args.warmup):
             step_device()
@@ -441,17 +711,12 @@ def main():
             "step_gbs": b_alg / (ms_step * 1e-3) / 1e9,
             "kernel_gbs": (b_kernel / (k_avg * 1e-3) / 1e9) if k_avg else None,
             "clocks": csum,
-            "tiled_plan": ({"ring_parts": plan[0], "chunk_vis": plan[1]}
-                           if plan else "automatic"),
+            "tiled_plan": plan if plan else "automatic",
         }
         if form == forms[0]:
             clock_summary = csum
 
     head = results[forms[0]]
-    def use_form(form):
-        g.set_precision(hpg_b200.PRECISION_MIXED if form == "mixed"
-                        else hpg_b200.PRECISION_FP64)
-        g.set_tiled_plan(*(plans.get(form) or (0, 0)))
 
     # end to end, every form: at least 10 pipelined steps, so that the first
     # step's unoverlapped copy and the last step's drain weigh little
@@ -459,22 +724,21 @@ def main():
     e2e_steps = max(10, args.steps)
     if not args.no_e2e:
         for form in forms:
-            use_form(form)
+            use_form(form, plans.get(form))
             run_e2e(2)
             ms_e2e = timed(lambda: run_e2e(e2e_steps), 1)
             results[form]["e2e"] = total_vis / (ms_e2e / e2e_steps * 1e-3) / 1e6
             results[form]["e2e_steps"] = e2e_steps
         e2e_value = results[forms[0]]["e2e"]
 
-    # full-size error of the mixed form against the FP64 form (one step each
+    # full-size error of the mixed forms against the FP64 form (one step each
     # from a zero grid; the FP64 form is checked against the CPU oracle by
-    # the parity tests)
+    # the parity tests and the parity field)
     mixed_err = None
     if "mixed" in results and "fp64" in results:
         grids = {}
-        for form in ("fp64", "mixed"):
-            g.set_precision(hpg_b200.PRECISION_MIXED if form == "mixed"
-                            else hpg_b200.PRECISION_FP64)
+        for form in [f for f in ("fp64", "mixed", "mixed-comp") if f in results]:
+            use_form(form, plans.get(form))
             g.reset_grid()
             # the same step, returning the residual visibilities into a copy
             # of the batch
@@ -485,17 +749,19 @@ def main():
                                 abi.visdata_dtype(4))["vis"]
             grids[form] = (g.grid_values(), g.grid_weights(), res)
             del dres
-        gf, wf, rf = grids["fp64"]
-        gm, wm, rm = grids["mixed"]
-        mixed_err = {
-            "grid_rel": float(np.linalg.norm((gm - gf).ravel()) /
-                              np.linalg.norm(gf.ravel())),
-            "weights_rel": float(np.linalg.norm(wm - wf) / np.linalg.norm(wf)),
-            "residual_vis_rel": float(
-                np.linalg.norm((rm.astype(np.complex128) - rf).ravel()) /
-                np.linalg.norm(rf.astype(np.complex128).ravel())),
-        }
-        del grids, gf, gm, rf, rm
+        gf, wf, rf = grids.pop("fp64")
+        mixed_err = {}
+        for form, (gm, wm, rm) in grids.items():
+            mixed_err[form] = {
+                "grid_rel": float(np.linalg.norm((gm - gf).ravel()) /
+                                  np.linalg.norm(gf.ravel())),
+                "weights_rel": float(np.linalg.norm(wm - wf) /
+                                     np.linalg.norm(wf)),
+                "residual_vis_rel": float(
+                    np.linalg.norm((rm.astype(np.complex128) - rf).ravel()) /
+                    np.linalg.norm(rf.astype(np.complex128).ravel())),
+            }
+        del grids, gf, rf
 
     cpu = None
     parity = None
@@ -513,7 +779,7 @@ def main():
         if oracle_out is not None:
             parity = {}
             for form in forms:
-                use_form(form)
+                use_form(form, plans.get(form))
                 parity[form] = device_parity(g, vis, oracle_out, form)
 
     if rank == 0:
@@ -527,9 +793,10 @@ def main():
             "data": "synthetic",
             "config": config_of(args, world, forms[0]),
             "forms": results,
-            "mixed_over_fp64": (results["mixed"]["value"] /
-                                results["fp64"]["value"]
-                                if len(results) == 2 else None),
+            "mixed_over_fp64": ({f: results[f]["value"] /
+                                 results["fp64"]["value"]
+                                 for f in results if f != "fp64"}
+                                if "fp64" in results else None),
             "mixed_vs_fp64_error": mixed_err,
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": int(vis.nbytes),

@@ -7,9 +7,10 @@ Python binding (``Gridder``, mirroring hpg::Gridder).
 from .abi import (HpgError, device_count, load, visdata_dtype,  # noqa: F401
                   FFT_NEGATIVE, FFT_POSITIVE, SHIFT_BACKWARD, SHIFT_FORWARD,
                   PRECISION_FP64, PRECISION_MIXED)
-from .gridder import CFArray, Future, Gridder  # noqa: F401
+from .gridder import (CFArray, Future, Gridder,  # noqa: F401
+                      grid_visibilities_batch)
 
 __all__ = ["HpgError", "device_count", "load", "visdata_dtype", "CFArray",
-           "Future", "Gridder", "FFT_NEGATIVE", "FFT_POSITIVE",
+           "Future", "Gridder", "grid_visibilities_batch", "FFT_NEGATIVE", "FFT_POSITIVE",
            "SHIFT_BACKWARD", "SHIFT_FORWARD", "PRECISION_FP64",
            "PRECISION_MIXED"]

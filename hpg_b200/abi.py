@@ -140,6 +140,8 @@ SIGNATURES = {
     "hpgb_last_gridding_kernel": ([_P, ctypes.POINTER(ctypes.c_int)], _I),
     "hpgb_set_tiled_plan_ex": ([_P, ctypes.c_void_p], _I),
     "hpgb_set_wait_limit": ([_P, ctypes.c_double], _I),
+    "hpgb_grid_visibilities_batch": ([_P, ctypes.c_size_t, _P, _P, ctypes.c_uint,
+                                      ctypes.c_uint, _I, _P], _I),
     "hpgb_debug_withhold_copy": ([_P, ctypes.c_longlong], _I),
     "hpgb_get_tiled_plan": ([_P, ctypes.c_void_p], _I),
     "hpgb_autotune_tiled": ([_P, _P, _S, _U, _U, _I, ctypes.POINTER(_I),

@@ -75,8 +75,11 @@ def build_device(verbose=False, force=False):
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(compile_one, sources))
     tmp = target + ".tmp"
+    # --no-undefined: a declaration without a definition fails the build
+    # here instead of the library's load on the device
     _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs +
          ["-L" + os.path.join(CUDA_HOME, "lib64"), "-lcufft",
+          "-Xlinker", "--no-undefined",
           "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64")])
     os.replace(tmp, target)
     return target

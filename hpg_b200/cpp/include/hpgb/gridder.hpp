@@ -214,6 +214,11 @@ class Gridder {
   // choice of arithmetic and kernels (no counterpart in the reference)
   opt_error_t set_precision(int precision);
   opt_error_t set_gridding_kernel(int kind);
+  // the tiled kernel's plan (hpgb_set_tiled_plan_ex) and the kernel that
+  // took the last batch (hpgb_last_gridding_kernel)
+  opt_error_t set_tiled_plan(const hpgb_tiled_plan& plan);
+  hpgb_tiled_plan tiled_plan() const;
+  int last_gridding_kernel() const;
 
   size_t convolution_function_region_size(const CFArrayShape* shape) const noexcept;
   opt_error_t allocate_convolution_function_region(const CFArrayShape* shape);
@@ -288,5 +293,33 @@ class Gridder {
 
 // the error of a status code (nullopt for success)
 opt_error_t error_of(int status);
+
+// The batches of many gridders in one launch of the tiled kernel
+// (hpgb_grid_visibilities_batch; no counterpart in the reference):
+// gridders[j] grids batches[j] as its grid_visibilities /
+// degrid_grid_visibilities would.  The gridders share polarizations, grid
+// rows, Mueller tables and arithmetic form; grids, CFs and batch sizes may
+// differ.  The work runs on gridders[0]'s stream; fence it for the results.
+template <typename V>
+opt_error_t grid_visibilities_batch(const std::vector<Gridder*>& gridders,
+                                    std::vector<std::vector<V>>& batches,
+                                    bool do_degrid = false,
+                                    bool update_grid_weights = true) {
+  if (gridders.size() != batches.size())
+    return Error("one batch per gridder", ErrorType::Other);
+  std::vector<hpgb_gridder*> hs;
+  std::vector<const void*> vs;
+  std::vector<size_t> ns;
+  for (size_t j = 0; j < gridders.size(); ++j) {
+    hs.push_back(gridders[j]->handle());
+    vs.push_back(batches[j].data());
+    ns.push_back(batches[j].size());
+  }
+  const unsigned flags = HPGB_DO_GRID | (do_degrid ? HPGB_DO_DEGRID : 0) |
+                         (update_grid_weights ? HPGB_UPDATE_GRID_WEIGHTS : 0);
+  return error_of(hpgb_grid_visibilities_batch(
+      hs.data(), hs.size(), vs.data(), ns.data(), VisNpol<V>::value, flags, 0,
+      nullptr));
+}
 
 }  // namespace hpgb

@@ -102,6 +102,22 @@ opt_error_t Gridder::set_gridding_kernel(int kind) {
   return error_of(hpgb_set_gridding_kernel(m_h, kind));
 }
 
+opt_error_t Gridder::set_tiled_plan(const hpgb_tiled_plan& plan) {
+  return error_of(hpgb_set_tiled_plan_ex(m_h, &plan));
+}
+
+hpgb_tiled_plan Gridder::tiled_plan() const {
+  hpgb_tiled_plan p{0, 0, 0, 0};
+  hpgb_get_tiled_plan(m_h, &p);
+  return p;
+}
+
+int Gridder::last_gridding_kernel() const {
+  int k = HPGB_KERNEL_AUTO;
+  hpgb_last_gridding_kernel(m_h, &k);
+  return k;
+}
+
 namespace {
 std::vector<unsigned> shape_extents(const CFArrayShape* s) {
   std::vector<unsigned> ext;

@@ -812,6 +812,110 @@ int hpgb_get_tiled_plan(const hpgb_gridder* g, hpgb_tiled_plan* plan) {
   });
 }
 
+int hpgb_grid_visibilities_batch(hpgb_gridder* const* gridders, size_t num,
+                                 const void* const* vis, const size_t* nvis,
+                                 unsigned npol, unsigned flags,
+                                 int vis_on_device, void* const* returned) {
+  return guarded([&]() -> Status {
+    if (!gridders || !vis || !nvis || num == 0)
+      return Status::err(HPGB_ERROR_OTHER, "null argument");
+    if (num > 96)
+      return Status::err(HPGB_ERROR_OTHER, "at most 96 gridders per batch");
+    hpgb_gridder* g0 = gridders[0];
+    if (!g0) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+    const bool do_grid = flags & HPGB_DO_GRID;
+    const bool ret = flags & HPGB_RETURN_VISIBILITIES;
+    for (size_t j = 0; j < num; ++j) {
+      hpgb_gridder* g = gridders[j];
+      if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");
+      for (size_t i = 0; i < j; ++i)
+        if (gridders[i] == g)
+          return Status::err(HPGB_ERROR_OTHER, "a gridder appears twice");
+      // validation order of src/hpg_runtime.hpp:1816-1828, per gridder
+      if (nvis[j] > g->max_batch)
+        return Status::err(HPGB_ERROR_EXCESSIVE_NUMBER_VISIBILITIES,
+                           "Number of visibilities exceeds maximum batch size");
+      if (npol != g->npol)
+        return Status::err(HPGB_ERROR_INVALID_NUMBER_POLARIZATIONS,
+                           "Number of visibility polarizations does not match "
+                           "Mueller matrix");
+      if (!do_grid && (flags & HPGB_UPDATE_GRID_WEIGHTS))
+        return Status::err(HPGB_ERROR_UPDATE_WEIGHTS_WITHOUT_GRIDDING,
+                           "Unable to update grid weights during degridding only");
+      if (nvis[j] > 0 && !vis[j])
+        return Status::err(HPGB_ERROR_OTHER, "null visibilities");
+      if (ret && nvis[j] > 0 && (!returned || !returned[j]))
+        return Status::err(HPGB_ERROR_OTHER,
+                           "null buffer for returned visibilities");
+      if (!g->cf.set)
+        return Status::err(HPGB_ERROR_OTHER, "no convolution function set");
+      HPGB_TRY(validate_mueller(g));
+      bool same = g->device == g0->device &&
+                  g->grid_size[2] == g0->grid_size[2] &&
+                  g->precision == g0->precision &&
+                  g->tplan.compensated == g0->tplan.compensated &&
+                  (!(flags & HPGB_DO_DEGRID) || g->has_model == g0->has_model);
+      for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c)
+          same = same && g->mt.m[r][c] == g0->mt.m[r][c] &&
+                 g->mt.c[r][c] == g0->mt.c[r][c];
+      if (!same)
+        return Status::err(HPGB_ERROR_OTHER,
+                           "the gridders of a batch must share their device, "
+                           "grid rows, Mueller tables, precision, compensation "
+                           "and (when degridding) whether a model is set");
+    }
+    if (!(flags & (HPGB_DO_DEGRID | HPGB_DO_GRID))) return Status::ok();
+    HPGB_CUDA_TRY(cudaSetDevice(g0->device));
+    const cudaStream_t st = g0->stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    HPGB_CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+    const bool capturing = cap != cudaStreamCaptureStatusNone;
+    // the others' queued work comes first
+    if (!capturing)
+      for (size_t j = 1; j < num; ++j) {
+        cudaEvent_t e;
+        HPGB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        cudaEventRecord(e, gridders[j]->stream);
+        cudaStreamWaitEvent(st, e, 0);
+        cudaEventDestroy(e);
+      }
+    const size_t rec = visdata_size(npol);
+    std::vector<void*> dvis(num, nullptr);
+    for (size_t j = 0; j < num; ++j) {
+      hpgb_gridder* g = gridders[j];
+      if (!vis_on_device && nvis[j] > 0)
+        HPGB_TRY(validate_indexes(g, vis[j], nvis[j]));
+      HPGB_TRY(g->vb.vis.reserve(std::max<size_t>(g->max_batch, 1) * rec));
+      dvis[j] = g->vb.vis.ptr;
+      if (nvis[j] > 0)
+        HPGB_CUDA_TRY(cudaMemcpyAsync(
+            dvis[j], vis[j], nvis[j] * rec,
+            vis_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+            st));
+    }
+    HPGB_TRY(grid_batch_tiled(gridders, num, dvis.data(), nvis, flags));
+    for (size_t j = 0; j < num; ++j) {
+      if (nvis[j] > 0) gridders[j]->last_kernel = HPGB_KERNEL_TILED;
+      if (ret && nvis[j] > 0)
+        HPGB_CUDA_TRY(cudaMemcpyAsync(
+            returned[j], dvis[j], nvis[j] * rec,
+            vis_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+            st));
+    }
+    // work queued on the others later comes after the batch
+    if (!capturing) {
+      cudaEvent_t e;
+      HPGB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      HPGB_CUDA_TRY(cudaEventRecord(e, st));
+      for (size_t j = 1; j < num; ++j)
+        cudaStreamWaitEvent(gridders[j]->stream, e, 0);
+      cudaEventDestroy(e);
+    }
+    return Status::ok();
+  });
+}
+
 int hpgb_set_wait_limit(hpgb_gridder* g, double seconds) {
   return guarded([&]() -> Status {
     if (!g) return Status::err(HPGB_ERROR_OTHER, "null gridder");

@@ -27,8 +27,9 @@
 // Visibilities whose footprint leaves the grid contribute nothing (the
 // reference skips them).  Grid-shaped arrays use the gridder's device grid
 // layout, double2 [cube][mrow][y][x]; per-visibility arrays are
-// double2 [n][npol].  One CTA per visibility; grid outputs are accumulated
-// with FP64 atomics.
+// double2 [n][npol].  The kernels here take one CTA per visibility and
+// accumulate grid outputs with FP64 global atomics; adjoint_tiled.cu runs
+// the same operators on the tile sort of the batch (the default).
 
 #include "gridder.cuh"
 
@@ -261,6 +262,20 @@ Status linear_op(hpgb_gridder* g, const void* d_vis, size_t n, int op,
   if (n > size_t(0x7fffffff))
     return Status::err(HPGB_ERROR_EXCESSIVE_NUMBER_VISIBILITIES,
                        "too many visibilities for one launch");
+  // the tile-sorted kernels (adjoint_tiled.cu) unless the per-visibility
+  // kernels are selected or the CF's region does not fit shared memory
+  if (g->kernel_kind != HPGB_KERNEL_DIRECT) {
+    bool used = false;
+    HPGB_TRY(linear_op_tiled(g, d_vis, n, op, in, out, &used));
+    if (used) {
+      g->last_kernel = HPGB_KERNEL_TILED;
+      return Status::ok();
+    }
+    if (g->kernel_kind == HPGB_KERNEL_TILED)
+      return Status::err(HPGB_ERROR_OTHER,
+                         "the tiled operators cannot take this CF or grid");
+  }
+  g->last_kernel = HPGB_KERNEL_DIRECT;
   switch (g->npol) {
     case 1: return linear_n<1>(g, d_vis, n, op, in, out);
     case 2: return linear_n<2>(g, d_vis, n, op, in, out);

@@ -1,0 +1,184 @@
+// grid_batch.cu -- one launch of the tiled kernel over the batches of many
+// gridders (hpgb_grid_visibilities_batch): many independent grids of
+// uneven sizes, each with its own CF set and batch, in one persistent
+// launch, so that the device stays full however small each job is and the
+// whole step is one kernel (and one CUDA graph).
+//
+// Every gridder's batch is sorted into uv tiles on its own buffers
+// (tiles.cuh), with the tile side its own CF allows under the launch's
+// common shared-memory plan; a small kernel then concatenates the gridders'
+// tile-pass lists into one work list, each pass tagged with its gridder,
+// and the tiled kernel reads each pass's grid, weights, CF, records, tile
+// geometry and model tensor map from a job table in device memory
+// (BatchJob).  All of it runs on the first gridder's stream; the others'
+// streams are ordered before and after it.  The gridders must share the
+// number of polarizations and grid rows, the Mueller tables, the arithmetic
+// form and (when degridding) whether a model is set.
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "tiled_kernel.cuh"
+
+namespace hpgb {
+
+using namespace tiled;
+
+namespace {
+
+struct ChunkSrc {
+  const Chunk* chunks;
+  const unsigned* num_chunks;
+};
+
+// The job table and the gridders' pass lists travel as the parameters of
+// the kernel that places them (kernel parameters are copied at launch, and
+// by value into a CUDA graph that captures the call): no host buffer has to
+// outlive the call.  BatchJob entries are carried as raw 16-byte words.
+struct BatchTable {
+  int njobs;
+  int pad[3];
+  ChunkSrc src[kMaxBatchJobs];
+  uint4 jobs[kMaxBatchJobs * sizeof(BatchJob) / 16];
+};
+static_assert(sizeof(BatchJob) % 16 == 0, "BatchJob is whole 16-byte words");
+static_assert(sizeof(BatchTable) <= 32000, "kernel parameter limit");
+
+// block j writes gridder j's job-table entry and copies its tile passes
+// behind those of gridders < j, tagged with j; the last block writes the
+// total
+__global__ void place_batch_kernel(const __grid_constant__ BatchTable t,
+                                   BatchJob* jobs, Chunk* out,
+                                   unsigned* total) {
+  const int j = blockIdx.x;
+  constexpr int kWords = int(sizeof(BatchJob) / 16);
+  uint4* dst = reinterpret_cast<uint4*>(jobs + j);
+  for (int w = threadIdx.x; w < kWords; w += blockDim.x)
+    dst[w] = t.jobs[j * kWords + w];
+  unsigned off = 0;
+  for (int i = 0; i < j; ++i) off += *t.src[i].num_chunks;
+  const unsigned nj = *t.src[j].num_chunks;
+  for (unsigned k = threadIdx.x; k < nj; k += blockDim.x) {
+    Chunk c = t.src[j].chunks[k];
+    c.pad = j;
+    out[off + k] = c;
+  }
+  if (j == t.njobs - 1 && threadIdx.x == 0) *total = off + nj;
+}
+
+template <bool MIXED>
+Status launch_batch_n(hpgb_gridder* g0, unsigned npol, const TiledParams& p,
+                      int smem, const CUtensorMap& map) {
+  switch (npol) {
+    case 1: return launch_tiled_kernel<1, MIXED, true>(g0, p, smem, map);
+    case 2: return launch_tiled_kernel<2, MIXED, true>(g0, p, smem, map);
+    case 3: return launch_tiled_kernel<3, MIXED, true>(g0, p, smem, map);
+    case 4: return launch_tiled_kernel<4, MIXED, true>(g0, p, smem, map);
+    default: return Status::err(HPGB_ERROR_OTHER, "bad polarization count");
+  }
+}
+
+}  // namespace
+
+Status grid_batch_tiled(hpgb_gridder* const* gs, size_t njobs,
+                        void* const* d_vis, const size_t* nvis,
+                        unsigned flags) {
+  hpgb_gridder* g0 = gs[0];
+  const cudaStream_t st = g0->stream;
+  const bool mixed = g0->precision == HPGB_PRECISION_MIXED;
+  BatchShape shape{0, 0};
+  size_t total = 0;
+  for (size_t j = 0; j < njobs; ++j) {
+    for (const CFGroup& G : gs[j]->cf.groups)
+      shape.max_plane_bytes = std::max(shape.max_plane_bytes, G.plane_stride * 8);
+    shape.max_taps = std::max(
+        shape.max_taps, std::max(gs[j]->cf.max_taps_x, gs[j]->cf.max_taps_y));
+    total += nvis[j];
+  }
+  if (total == 0) return Status::ok();
+  if (total > size_t(0x7fffffff))
+    return Status::err(HPGB_ERROR_EXCESSIVE_NUMBER_VISIBILITIES,
+                       "too many visibilities for one launch");
+  const Plan plan = make_plan(g0, flags, mixed, total, &shape);
+  if (!plan.ok)
+    return Status::err(HPGB_ERROR_OTHER,
+                       "the tiled kernel cannot take this batch: " + plan.why);
+  const int R = plan.R;
+  if (njobs > size_t(kMaxBatchJobs))
+    return Status::err(HPGB_ERROR_OTHER, "more gridders than one launch takes");
+  std::vector<BatchJob> jobs(njobs);
+  std::vector<ChunkSrc> srcs(njobs);
+  size_t max_chunks = 0;
+  const bool model = plan.p.do_degrid && plan.p.has_model;
+  // every model's rows must start on 16-byte boundaries for its tensor map
+  // (an odd grid width in the mixed form's FP32 copy does not)
+  if (model)
+    for (size_t j = 0; j < njobs; ++j)
+      if ((2 * size_t(gs[j]->grid_size[0]) * (mixed ? 4 : 8)) % 16 != 0)
+        return Status::err(HPGB_ERROR_OTHER,
+                           "gridder " + std::to_string(j) +
+                               ": model row pitch not a 16-byte multiple "
+                               "(odd grid width in the mixed form)");
+  for (size_t j = 0; j < njobs; ++j) {
+    hpgb_gridder* g = gs[j];
+    BatchJob& b = jobs[j];
+    std::memset(&b, 0, sizeof(b));
+    const int taps = std::max(g->cf.max_taps_x, g->cf.max_taps_y);
+    // the largest tile this gridder's CF allows in the launch's region
+    b.T = R - taps + 1;
+    b.nx = int(g->grid_size[0]);
+    b.ny = int(g->grid_size[1]);
+    b.ntx = (b.nx + b.T - 1) / b.T;
+    b.nty = (b.ny + b.T - 1) / b.T;
+    b.cf = g->cf.data.as<const float2>();
+    b.grid = g->grid.as<double2>();
+    b.weights = g->weights.as<double>();
+    b.records = static_cast<unsigned char*>(d_vis[j]);
+    if (nvis[j] > 0) {
+      TilePrep prep;
+      HPGB_TRY(prepare_tiles(g, d_vis[j], nvis[j], b.T, b.ntx, b.nty, plan.K,
+                             &prep, st));
+      b.descs = prep.descs;
+      b.srefs = prep.srefs;
+      srcs[j] = ChunkSrc{prep.chunks, prep.num_chunks};
+      max_chunks += prep.max_chunks;
+    } else {
+      // no passes: point at a zero count
+      srcs[j] = ChunkSrc{nullptr, g->vb.counters.as<unsigned>() + 3};
+      HPGB_CUDA_TRY(cudaMemsetAsync(g->vb.counters.as<unsigned>() + 3, 0,
+                                    sizeof(unsigned), st));
+    }
+    if (model) HPGB_TRY(encode_model_map(g, mixed, R, &b.model_map, st));
+  }
+  // job table and the combined work list, in g0's buffers
+  VisBuffers& vb = g0->vb;
+  HPGB_TRY(vb.batch_jobs.reserve(njobs * sizeof(BatchJob)));
+  HPGB_TRY(vb.batch_chunks.reserve(std::max<size_t>(max_chunks, 1) * sizeof(Chunk)));
+  std::unique_ptr<BatchTable> table(new BatchTable);
+  std::memset(table.get(), 0, sizeof(BatchTable));
+  table->njobs = int(njobs);
+  std::memcpy(table->src, srcs.data(), njobs * sizeof(ChunkSrc));
+  std::memcpy(table->jobs, jobs.data(), njobs * sizeof(BatchJob));
+  unsigned* total_chunks = vb.counters.as<unsigned>() + 4;
+  place_batch_kernel<<<unsigned(njobs), 128, 0, st>>>(
+      *table, vb.batch_jobs.as<BatchJob>(), vb.batch_chunks.as<Chunk>(),
+      total_chunks);
+  HPGB_CUDA_TRY(cudaGetLastError());
+  ++g0->launches;
+  TiledParams p = plan.p;
+  p.jobs = vb.batch_jobs.as<const BatchJob>();
+  p.chunks = vb.batch_chunks.as<Chunk>();
+  p.num_chunks = total_chunks;
+  p.rec_stride = int(visdata_size(g0->npol));
+  p.status = vb.counters.as<unsigned>();
+  p.wait_limit_ns = g0->wait_limit_ns;
+  p.withhold_vis = g0->withhold_vis;
+  CUtensorMap unused;
+  std::memset(&unused, 0, sizeof(unused));
+  if (mixed) return launch_batch_n<true>(g0, g0->npol, p, plan.smem, unused);
+  return launch_batch_n<false>(g0, g0->npol, p, plan.smem, unused);
+}
+
+}  // namespace hpgb

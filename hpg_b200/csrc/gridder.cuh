@@ -46,6 +46,8 @@ struct VisBuffers {
   // tiled path: sorted work description
   DevBuf keys, keys_alt, order, order_alt, sort_tmp, buckets, items, counters;
   DevBuf prep;      // per-visibility prepared records (sorted order)
+  // batched launches led by this gridder: job table and combined pass list
+  DevBuf batch_jobs, batch_chunks;
   // host batches outside a stream capture: two staging buffers, used in
   // turn, so that one call's host->device copy overlaps the previous call's
   // work
@@ -143,6 +145,11 @@ Status grid_tiled(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
 bool tiled_plan_side(const hpgb_gridder* g, unsigned flags, size_t n,
                      int* side);
 
+// grid_batch.cu: one tiled launch over the device batches of many gridders
+// (validated by the caller: same polarizations, rows, Mueller tables, form)
+Status grid_batch_tiled(hpgb_gridder* const* gs, size_t njobs,
+                        void* const* d_vis, const size_t* nvis, unsigned flags);
+
 // autotune.cu: times tiled plans on the batch, keeps the fastest
 Status autotune_tiled(hpgb_gridder* g, const void* vis, size_t n,
                       unsigned flags, bool on_device, int* best_ring,
@@ -165,6 +172,10 @@ Status debug_coords(hpgb_gridder* g, const void* d_vis, size_t n,
 // values)
 Status linear_op(hpgb_gridder* g, const void* d_vis, size_t n, int op,
                  const void* in, void* out);
+// adjoint_tiled.cu: the same on the tile sort of the batch; *used is false
+// when the CF's tile region does not fit shared memory
+Status linear_op_tiled(hpgb_gridder* g, const void* d_vis, size_t n, int op,
+                       const void* in, void* out, bool* used);
 
 // imaging.cu
 Status normalize_by_weights(hpgb_gridder* g, double wfactor);

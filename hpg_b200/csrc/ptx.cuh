@@ -62,11 +62,12 @@ __device__ __forceinline__ void mbar_arrive_remote(uint64_t* bar,
 constexpr uint32_t kSuspendHintNs = 20000;
 constexpr uint64_t kWaitLimitNs = 500000000ull;  // default limit: 0.5 s
 
-// The CTA's wait-control block in shared memory: the abort flag, then (8
-// bytes further) the wait limit in nanoseconds.  Waits take its address.
+// The CTA's wait-control block in shared memory: the abort flag, a count of
+// the tensor copies issued (for the drain before exit), then (8 bytes in)
+// the wait limit in nanoseconds.  Waits take the flag's address.
 struct WaitCtl {
   int flag;
-  int pad;
+  int copies;
   unsigned long long limit_ns;
 };
 

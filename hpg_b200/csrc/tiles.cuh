@@ -57,8 +57,8 @@ struct TilePrep {
 
 // Sorts the batch d_vis (n VisData<npol> records in device memory) into
 // tiles of T x T origins, ntx x nty tiles per grid cube, passes of at most
-// K visibilities; all on the gridder's stream.
+// K visibilities; all on stream st (the gridder's stream when null).
 Status prepare_tiles(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
-                     int nty, int K, TilePrep* out);
+                     int nty, int K, TilePrep* out, cudaStream_t st = nullptr);
 
 }  // namespace hpgb

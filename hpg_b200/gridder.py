@@ -467,3 +467,51 @@ class _Capture:
         elif rc == 0 and h:
             load().hpgb_graph_destroy(h)
         return False
+
+
+def grid_visibilities_batch(gridders, visibilities, update_grid_weights=True,
+                            do_degrid=False, return_visibilities=False,
+                            on_device=False):
+    """The batches of many gridders in one launch of the tiled kernel
+    (hpgb_grid_visibilities_batch): gridders[j] grids visibilities[j] as
+    its own grid_visibilities / degrid_grid_visibilities call would.  With
+    return_visibilities, returns one Future per gridder (resolved by
+    gridders[0].fence()).  Host record arrays, or CUDA uint8 tensors with
+    on_device."""
+    n = len(gridders)
+    if n == 0 or len(visibilities) != n:
+        raise ValueError("one batch per gridder")
+    npol = gridders[0].npol
+    rec = abi.visdata_dtype(npol).itemsize
+    flags = abi.DO_GRID | (abi.UPDATE_GRID_WEIGHTS if update_grid_weights else 0)
+    if do_degrid:
+        flags |= abi.DO_DEGRID
+    if return_visibilities:
+        flags |= abi.RETURN_VISIBILITIES
+    keep, outs = [], []
+    hs = (ctypes.c_void_p * n)(*[g._h.value if hasattr(g._h, "value") else g._h
+                                 for g in gridders])
+    vp = (ctypes.c_void_p * n)()
+    nv = (ctypes.c_size_t * n)()
+    rp = (ctypes.c_void_p * n)()
+    for j, v in enumerate(visibilities):
+        if on_device:
+            nv[j] = v.numel() * v.element_size() // rec
+            vp[j] = v.data_ptr()
+            out = v if return_visibilities else None
+            if out is not None:
+                rp[j] = out.data_ptr()
+        else:
+            v = np.ascontiguousarray(v)
+            keep.append(v)
+            nv[j] = len(v)
+            vp[j] = v.ctypes.data
+            out = np.empty_like(v) if return_visibilities else None
+            if out is not None:
+                rp[j] = out.ctypes.data
+        outs.append(out)
+    check(load().hpgb_grid_visibilities_batch(
+        hs, n, vp, nv, npol, flags, 1 if on_device else 0, rp))
+    if return_visibilities:
+        return [Future(gridders[0], o) for o in outs]
+    return None

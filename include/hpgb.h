@@ -397,6 +397,30 @@ HPGB_API int hpgb_set_tiled_plan_ex(hpgb_gridder* gridder,
 HPGB_API int hpgb_get_tiled_plan(const hpgb_gridder* gridder,
                                  hpgb_tiled_plan* plan);
 
+/* State::grid_visibilities for the batches of many gridders in ONE launch
+ * of the tiled kernel, no counterpart in the reference (which launches per
+ * gridder).  Gridder j takes visibilities[j] (num_visibilities[j] records;
+ * host or device memory as vis_on_device says), exactly as
+ * hpgb_grid_visibilities(gridders[j], ..., flags, ...) would, and with
+ * HPGB_RETURN_VISIBILITIES writes its returned records to returned[j]
+ * (valid after hpgb_fence(gridders[0])).  Up to 96 distinct gridders on one
+ * device that share the number of polarizations, grid rows, Mueller tables,
+ * precision and compensation setting, and -- when degridding -- whether a
+ * model is set; grid sizes, CFs and batch sizes may all differ.  Every
+ * gridder's batch is sorted into uv tiles with the tile side its own CF
+ * allows, and the tile passes of all of them form one work list of one
+ * persistent launch.  The work runs on gridders[0]'s stream, ordered after
+ * the work already queued on the others' streams and before work queued on
+ * them later (outside a stream capture; inside one, the caller orders the
+ * other gridders' work).  Errors: those of hpgb_grid_visibilities, checked
+ * per gridder, and HPGB_ERROR_OTHER when the gridders differ in a shared
+ * property or the tiled kernel cannot take their CFs. */
+HPGB_API int hpgb_grid_visibilities_batch(
+    hpgb_gridder* const* gridders, size_t num_gridders,
+    const void* const* visibilities, const size_t* num_visibilities,
+    unsigned num_polarizations, unsigned flags, int vis_on_device,
+    void* const* returned);
+
 /* Bound of every device-side wait of the tiled kernel, in seconds (0.5 by
  * default; 1e-4..60), no counterpart in the reference.  A wait that runs out
  * ends the launch early with an error status: the next hpgb_fence returns

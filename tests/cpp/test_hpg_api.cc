@@ -160,6 +160,33 @@ int main() {
               hpgb::ErrorType::InvalidNumberMuellerIndexRows);
   }
 
+  // batched launch over two gridders of different sizes; plan controls
+  {
+    auto ra = hpgb::Gridder::create(0, 0, 4, {64, 64, 1, 1}, scale, {{0}}, {{0}});
+    auto rb = hpgb::Gridder::create(0, 0, 4, {96, 80, 1, 1}, scale, {{0}}, {{0}});
+    CHECK(hpgb::is_value(ra) && hpgb::is_value(rb));
+    hpgb::Gridder a = std::move(hpgb::get_value(ra));
+    hpgb::Gridder b = std::move(hpgb::get_value(rb));
+    CHECK(!a.set_convolution_function(cf) && !b.set_convolution_function(cf));
+    hpgb_tiled_plan plan{4, 64, 0, 0};
+    CHECK(!a.set_tiled_plan(plan));
+    CHECK(a.tiled_plan().ring_parts == 4 && a.tiled_plan().chunk_vis == 64);
+    std::vector<std::vector<hpgb::VisData<1>>> batches{
+        {one_vis(3.2, -7.6, {2.0f, 1.0f}, 0.5f)},
+        {one_vis(-5.1, 4.4, {1.0f, -1.0f}, 2.0f)}};
+    CHECK(!hpgb::grid_visibilities_batch<hpgb::VisData<1>>({&a, &b}, batches));
+    a.fence();
+    CHECK(a.last_gridding_kernel() == HPGB_KERNEL_TILED);
+    auto ga = a.grid_values();
+    auto gb = b.grid_values();
+    std::complex<double> sa = 0, sb = 0;
+    for (size_t i = 0; i < ga->size(); ++i) sa += ga->data()[i];
+    for (size_t i = 0; i < gb->size(); ++i) sb += gb->data()[i];
+    // taps^2 cells of vis * weight each
+    CHECK(std::abs(sa - double(taps * taps) * std::complex<double>(1.0, 0.5)) < 1e-12);
+    CHECK(std::abs(sb - double(taps * taps) * std::complex<double>(2.0, -2.0)) < 1e-12);
+  }
+
   if (failures == 0) std::printf("OK\n");
   return failures == 0 ? 0 : 1;
 }

@@ -8,7 +8,7 @@ alone recovers it.  The chunk starts at byte 4080 and inflates to
 91*91*16 bytes, row-major [x - 9523][y - 8522] (the test's indexing at
 GridderStateUnitTests.cc:1433-1438).
 
-    python tests/golden/make_gridone.py [path/to/gridone.h5]
+    python tests/golden/make_gridone.py path/to/hpg/tests/gridone.h5
 """
 import json
 import os
@@ -18,12 +18,11 @@ import zlib
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SRC = "/root/reference/tests/gridone.h5"
 CHUNK_OFFSET = 4080
 SHAPE = (91, 91)
 
 
-def main(src=DEFAULT_SRC):
+def main(src):
     raw = open(src, "rb").read()
     data = zlib.decompressobj().decompress(raw[CHUNK_OFFSET:])
     assert len(data) == SHAPE[0] * SHAPE[1] * 16, len(data)
@@ -50,4 +49,6 @@ def main(src=DEFAULT_SRC):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_gridone.py path/to/hpg/tests/gridone.h5")
+    main(sys.argv[1])

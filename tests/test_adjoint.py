@@ -19,12 +19,23 @@ from hpg_b200 import CFArray, Gridder, abi, workloads
 pytestmark = pytest.mark.gpu
 
 
-def setup(n=1500, grad=0.3, seed=21, model=True):
+KINDS = {"direct": abi.KERNEL_DIRECT, "tiled": abi.KERNEL_TILED}
+
+
+@pytest.fixture(params=["tiled", "direct"])
+def kind(request):
+    """The operators on the tile sort of the batch (adjoint_tiled.cu) and
+    the per-visibility kernels (adjoint.cu)."""
+    return request.param
+
+
+def setup(n=1500, grad=0.3, seed=21, model=True, kind="tiled"):
     import torch
     cfg = workloads.full_pol_config(n, grid=128, oversampling=16,
                                     supports=(4, 6, 8), seed=seed, grad=grad)
     g = Gridder.create(0, 0, n, None, cfg["grid_size"], cfg["grid_scale"],
                        cfg["mueller"], cfg["conj_mueller"])
+    g.set_gridding_kernel(KINDS[kind])
     g.set_convolution_function(CFArray(cfg["oversampling"], cfg["cf_extents"],
                                        cfg["cf_values"]))
     dvis = torch.from_numpy(
@@ -44,10 +55,10 @@ def grid_shape(cfg):
     return (nc, nr, ny, nx)
 
 
-def test_degrid_dot_product(gpu):
+def test_degrid_dot_product(gpu, kind):
     import torch
     from hpg_b200 import autograd as ag
-    cfg, g, dvis = setup()
+    cfg, g, dvis = setup(kind=kind)
     gen = torch.Generator(device="cuda:0").manual_seed(1)
     n = len(cfg["vis"])
     x = crandn(grid_shape(cfg), gen)
@@ -64,10 +75,10 @@ def test_degrid_dot_product(gpu):
     g.close()
 
 
-def test_grid_dot_product(gpu):
+def test_grid_dot_product(gpu, kind):
     import torch
     from hpg_b200 import autograd as ag
-    cfg, g, dvis = setup(seed=22)
+    cfg, g, dvis = setup(seed=22, kind=kind)
     gen = torch.Generator(device="cuda:0").manual_seed(2)
     n = len(cfg["vis"])
     u = crandn((n, 4), gen)
@@ -83,11 +94,11 @@ def test_grid_dot_product(gpu):
     g.close()
 
 
-def test_operators_match_gridder(gpu):
+def test_operators_match_gridder(gpu, kind):
     """D and G against the gridder's own degridding and gridding."""
     import torch
     from hpg_b200 import autograd as ag
-    cfg, g, dvis = setup(seed=23)
+    cfg, g, dvis = setup(seed=23, kind=kind)
     g.set_model(cfg["model"])
     fut = g.degrid_get_predicted_visibilities(cfg["vis"])
     g.fence()
@@ -105,13 +116,13 @@ def test_operators_match_gridder(gpu):
     g.close()
 
 
-def test_degrid_adjoint_is_oracle_gridding_of_cotangent(gpu, oracle_lib):
+def test_degrid_adjoint_is_oracle_gridding_of_cotangent(gpu, kind, oracle_lib):
     """D^H y is the reference's gridding (mueller == conjugate mueller here)
     of the values y * phasor / conj(den) / (phasor * w)."""
     import torch
     from hpg_b200 import autograd as ag
     O = oracle_lib
-    cfg, g, dvis = setup(n=800, seed=24)
+    cfg, g, dvis = setup(n=800, seed=24, kind=kind)
     vis = cfg["vis"]
     n = len(vis)
     rng = np.random.default_rng(5)
@@ -134,12 +145,12 @@ def test_degrid_adjoint_is_oracle_gridding_of_cotangent(gpu, oracle_lib):
     g.close()
 
 
-def test_loss_gradient_finite_differences(gpu):
+def test_loss_gradient_finite_differences(gpu, kind):
     """dL/dG of L = sum w |D(G) - V|^2 through torch.autograd against
     central differences on random grid cells."""
     import torch
     from hpg_b200 import autograd as ag
-    cfg, g, dvis = setup(n=600, seed=25)
+    cfg, g, dvis = setup(n=600, seed=25, kind=kind)
     n = len(cfg["vis"])
     gen = torch.Generator(device="cuda:0").manual_seed(3)
     G0 = crandn(grid_shape(cfg), gen, 0.1)
@@ -184,4 +195,74 @@ def test_operator_argument_errors(gpu):
     rc = lib.hpgb_grid_linear(g._h, ctypes.c_void_p(dvis.data_ptr()), 10, 4,
                               None, None)
     assert rc == 1 + abi.ERROR_TYPES.index("Other")
+    g.close()
+
+
+def test_tiled_operators_equal_direct(gpu):
+    """The tile-sorted operators against the per-visibility ones: the same
+    FP64 arithmetic in another summation order (1e-12)."""
+    import torch
+    from hpg_b200 import autograd as ag
+    cfg, gt, dvis = setup(n=1200, seed=27, kind="tiled")
+    _, gd, _ = setup(n=1200, seed=27, kind="direct")
+    gen = torch.Generator(device="cuda:0").manual_seed(4)
+    n = len(cfg["vis"])
+    x = crandn(grid_shape(cfg), gen)
+    y = crandn((n, 4), gen)
+    for op in (ag.Degrid, ag.Grid):
+        arg = x if op is ag.Degrid else y
+        a = op.apply(arg, gt, dvis)
+        b = op.apply(arg, gd, dvis)
+        assert gt.last_gridding_kernel() == abi.KERNEL_TILED
+        assert gd.last_gridding_kernel() == abi.KERNEL_DIRECT
+        assert torch.linalg.norm(a - b) / torch.linalg.norm(b) <= 1e-12
+        # adjoints
+        cot = y if op is ag.Degrid else x
+        ar = arg.clone().requires_grad_(True)
+        op.apply(ar, gt, dvis).backward(cot)
+        br = arg.clone().requires_grad_(True)
+        op.apply(br, gd, dvis).backward(cot)
+        assert (torch.linalg.norm(ar.grad - br.grad) /
+                torch.linalg.norm(br.grad)) <= 1e-12
+    gt.close()
+    gd.close()
+
+
+@pytest.mark.parametrize("npol,expect", [(1, abi.KERNEL_TILED),
+                                         (2, abi.KERNEL_TILED),
+                                         (4, abi.KERNEL_DIRECT)])
+def test_wide_support_dot_products(gpu, npol, expect):
+    """Supports 8..64 (9..65 taps), diagonal Mueller, as in the
+    differentiable workload: both dot-product identities.  One or two grid
+    rows take the tiled operators; four rows of FP64 regions for 65 taps do
+    not fit shared memory, and the automatic choice takes the per-visibility
+    kernels."""
+    import torch
+    from hpg_b200 import autograd as ag
+    rng = np.random.default_rng(50 + npol)
+    gs = (256, 256, npol, 1)
+    supports = (8, 24, 40, 64)
+    ext, vals = workloads.separable_cf(supports, 8, np.ones(npol) +
+                                       0.1j * rng.standard_normal(npol))
+    mi = [[r if c == r else -1 for c in range(npol)] for r in range(npol)]
+    vis = workloads.visibilities(2000, npol, gs, (0.05, 0.05), 1.4e9, rng,
+                                 disk=0.3, w_frac=0.3, ngroups=len(supports),
+                                 grad=0.2)
+    g = Gridder.create(0, 0, len(vis), None, gs, (0.05, 0.05), mi, mi)
+    g.set_gridding_kernel(abi.KERNEL_AUTO)
+    g.set_convolution_function(CFArray(8, ext, vals))
+    dvis = torch.from_numpy(
+        np.frombuffer(vis.tobytes(), np.uint8).copy()).to("cuda:0")
+    gen = torch.Generator(device="cuda:0").manual_seed(6)
+    x = crandn((1, npol, 256, 256), gen)
+    y = crandn((len(vis), npol), gen)
+    for op, arg, cot in ((ag.Degrid, x, y), (ag.Grid, y, x)):
+        fx = op.apply(arg, g, dvis)
+        ar = arg.clone().requires_grad_(True)
+        op.apply(ar, g, dvis).backward(cot)
+        lhs = torch.vdot(fx.flatten(), cot.flatten())
+        rhs = torch.vdot(arg.flatten(), ar.grad.flatten())
+        assert abs(lhs) > 0
+        assert abs(lhs - rhs) / abs(lhs) <= 1e-10
+        assert g.last_gridding_kernel() == expect
     g.close()

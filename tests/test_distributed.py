@@ -93,3 +93,71 @@ def test_two_rank_sharded_gridding_matches_one_process(oracle_lib):
         assert np.abs(o.grid).max() > 0
         assert np.linalg.norm(grid - o.grid) <= 1e-12 * np.linalg.norm(o.grid)
         np.testing.assert_allclose(weights, o.weights, rtol=1e-12)
+
+
+def _device_worker(rank, world, port, queue, precision):
+    """One rank: its own device gridder on cuda:0, its shard, the grids and
+    weights summed over gloo."""
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    try:
+        from datetime import timedelta
+        from hpg_b200 import CFArray, Gridder
+        dist.init_process_group("gloo", rank=rank, world_size=world,
+                                timeout=timedelta(seconds=120))
+        cfg = _config()
+
+        def grid_shard(vis_shard):
+            g = Gridder.create(0, 0, max(len(vis_shard), 1), None,
+                               cfg["grid_size"], cfg["grid_scale"],
+                               cfg["mueller"], cfg["conj_mueller"])
+            g.set_precision(precision)
+            g.set_convolution_function(CFArray(cfg["oversampling"],
+                                               cfg["cf_extents"],
+                                               cfg["cf_values"]))
+            g.grid_visibilities(vis_shard)
+            out = g.grid_values(), g.grid_weights()
+            g.close()
+            return out
+
+        grid, weights = D.grid_sharded(grid_shard, cfg["vis"])
+        queue.put((rank, grid, weights))
+        dist.destroy_process_group()
+    except Exception as e:  # reported to the parent, which fails the test
+        queue.put((rank, repr(e), None))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_two_rank_sharded_device_gridding(gpu, oracle_lib, precision):
+    """The same sharding with the device gridder on every rank (two
+    processes on one GPU, no kernel waits on another rank; the grids meet
+    in a gloo all-reduce of their complex128 arrays): equal to the oracle's
+    gridding of the whole batch (1e-12 FP64, 1e-6 mixed)."""
+    import multiprocessing as mp
+    from hpg_b200 import abi
+    prec = abi.PRECISION_FP64 if precision == 0 else abi.PRECISION_MIXED
+    ctx = mp.get_context("spawn")
+    queue = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_device_worker, args=(r, 2, port, queue, prec))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    results = {}
+    for _ in range(2):
+        rank, grid, weights = queue.get(timeout=300)
+        assert not isinstance(grid, str), grid
+        results[rank] = (grid, weights)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    cfg = _config()
+    o = _oracle(cfg)
+    o.grid_visibilities(cfg["vis"])
+    tol = 1e-12 if precision == 0 else 1e-6
+    for rank in (0, 1):
+        grid, weights = results[rank]
+        assert np.linalg.norm(grid - o.grid) <= tol * np.linalg.norm(o.grid)
+        np.testing.assert_allclose(weights, o.weights, rtol=1e-12)
