@@ -440,10 +440,11 @@ def run_batch(args):
     polarizations (diagonal Mueller), a batch log-uniform in [10k, 2M]
     visibilities (uv uniform in the disk), 1..16 CF groups with supports
     drawn from {8, 16, 32, 64} at oversampling 64; mixed form.  One step
-    grids every job's batch: the jobs of each polarization class go to one
-    hpgb_grid_visibilities_batch call (one persistent tiled launch per
-    class, three at most), device-resident inputs.  The same step is timed
-    with one call per job (one tiled launch each) beside it.  Prints one JSON line: Mvis/s of both, and the
+    grids every job's batch: the jobs of each polarization count go to one
+    hpgb_grid_visibilities_batch call, which takes one persistent tiled
+    launch per support class of its gridders (nine launches at most here),
+    device-resident inputs.  The same step is timed with one call per job
+    (one tiled launch each) beside it.  Prints one JSON line: Mvis/s of both, and the
     batched launches' HBM roofline (records + CF slices once per visibility
     + grid read/write per job)."""
     import torch
@@ -477,18 +478,21 @@ def run_batch(args):
         taps = np.asarray(taps_of(supports), np.int64)[
             vis["cf_index"][:, 1].astype(np.int64)]
         jobs.append(dict(g=g, dvis=dvis, npol=npol, nvis=nvis, side=side,
+                         max_support=max(supports),
                          bytes=int(len(vis) * vis.dtype.itemsize +
                                    (taps * taps).sum() * npol * 8 +
                                    2 * side * side * npol * 16)))
         del vis
     torch.cuda.empty_cache()
+    # one batched call per polarization class (the library splits each by
+    # the gridders' widest CF into one launch per support class)
     classes = {}
     for job in jobs:
         classes.setdefault(job["npol"], []).append(job)
     total_vis = sum(j["nvis"] for j in jobs)
     total_bytes = sum(j["bytes"] for j in jobs)
-    def batched():
-        for cls in classes.values():
+    def batched(groups):
+        for cls in groups.values():
             hpg_b200.grid_visibilities_batch(
                 [j["g"] for j in cls], [j["dvis"] for j in cls],
                 on_device=True)
@@ -518,11 +522,21 @@ def run_batch(args):
 
     # each class's launch runs on the stream of its first gridder, so the
     # classes may overlap; the step ends when every gridder's work has
-    ms_batched = timed(batched)
+    ms_batched = timed(lambda: batched(classes))
+    # each polarization class alone: its batched call against its jobs'
+    # own calls
+    per_class = {}
+    for k, cls in classes.items():
+        one = {k: cls}
+        mb = timed(lambda: batched(one))
+        ms = timed(lambda: [j["g"].grid_visibilities(j["dvis"], on_device=True)
+                            for j in cls])
+        per_class[f"{k}pol"] = {"jobs": len(cls),
+                                "vis": sum(j["nvis"] for j in cls),
+                                "batched_ms": mb, "per_job_ms": ms}
     for job in jobs:
         job["g"].set_gridding_kernel(abi.KERNEL_TILED)
     ms_single = timed(per_job)
-    launches = {k: len(v) for k, v in classes.items()}
     peak, peak_kind = peaks()
     line = {
         "metric": "Mvis/s gridding of 64 uneven jobs (batched launches)",
@@ -535,7 +549,14 @@ def run_batch(args):
                                f"vis, 1-16 CF groups of supports "
                                f"{{8,16,32,64}}, os {os_}",
                    "total_vis": total_vis,
-                   "jobs_per_polarization_class": launches},
+                   "batch_calls": len(classes),
+                   "jobs_per_call": {f"{k}pol": len(v)
+                                     for k, v in classes.items()},
+                   "launches": len({(j["npol"],
+                                     0 if j["max_support"] <= 16 else
+                                     1 if j["max_support"] <= 32 else 2)
+                                    for j in jobs})},
+        "per_class": per_class,
         "per_job_launches": {"value": total_vis / (ms_single * 1e-3) / 1e6,
                              "ms_per_step": ms_single},
         "roofline": {"bound": "hbm", "achieved": total_bytes /

@@ -55,6 +55,8 @@ struct AdjParams {
   const double2* grid_in;  // gathers: model / grid cotangent
   double2* grid_out;       // scatters: accumulated
   const double2* vals_in;  // scatters: [n][npol]
+  int scatter_cta;  // scatters: the CTA on one visibility at a time (1) or a
+                    // warp per visibility with shared-memory atomics (0)
   double2* vals_out;       // gathers: [n][npol]
 };
 
@@ -95,7 +97,12 @@ __device__ __forceinline__ AdjVis adj_vis(const TileDesc* d, const SliceRef* s) 
 // HBM reads in flight -- the slices stream from HBM once, nothing to
 // reuse).  GATHER: acc += CF' * (region * screen) per polarization;
 // otherwise region += screen * sum_q CF' * a[q] with shared-memory atomics.
-template <int N, bool GATHER, bool SCREEN>
+// STRIDE threads share the visibility's cells (a warp, or the whole CTA);
+// ATOMIC: scatters add with shared-memory atomics (a warp per visibility,
+// footprints of concurrent visibilities may overlap) or with plain
+// read-modify-writes (the CTA on one visibility at a time: no two threads
+// touch a cell).
+template <int N, bool GATHER, bool SCREEN, int STRIDE, bool ATOMIC>
 __device__ __forceinline__ void vis_cells(const AdjVis& v, const int (*mi)[4],
                                           double im, const float2* slice,
                                           double2* region, int R, int RR,
@@ -105,12 +112,12 @@ __device__ __forceinline__ void vis_cells(const AdjVis& v, const int (*mi)[4],
   constexpr int U = (!SCREEN && N <= 2) ? 8 : 4;
   const int ncell = v.tx * v.ty;
   const double sph = GATHER ? -1.0 : 1.0;
-  for (int base = lane; base < ncell; base += 32 * U) {
+  for (int base = lane; base < ncell; base += STRIDE * U) {
     int rc[U];
     double2 s[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const int c = base + 32 * u;
+      const int c = base + STRIDE * u;
       const int cu = c < ncell ? c : 0;
       const int Y = cu / v.tx, X = cu - Y * v.tx;
       if constexpr (SCREEN) {
@@ -136,8 +143,9 @@ __device__ __forceinline__ void vis_cells(const AdjVis& v, const int (*mi)[4],
           float2 cf[U];
 #pragma unroll
           for (int u = 0; u < U; ++u)
-            cf[u] = base + 32 * u < ncell ? __ldg(plane + base + 32 * u)
-                                          : make_float2(0.f, 0.f);
+            cf[u] = base + STRIDE * u < ncell
+                        ? __ldg(plane + base + STRIDE * u)
+                        : make_float2(0.f, 0.f);
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             const double2 pr =
@@ -158,8 +166,9 @@ __device__ __forceinline__ void vis_cells(const AdjVis& v, const int (*mi)[4],
           float2 cf[U];
 #pragma unroll
           for (int u = 0; u < U; ++u)
-            cf[u] = base + 32 * u < ncell ? __ldg(plane + base + 32 * u)
-                                          : make_float2(0.f, 0.f);
+            cf[u] = base + STRIDE * u < ncell
+                        ? __ldg(plane + base + STRIDE * u)
+                        : make_float2(0.f, 0.f);
 #pragma unroll
           for (int u = 0; u < U; ++u)
             sum[u] = cadd_d(sum[u],
@@ -168,11 +177,16 @@ __device__ __forceinline__ void vis_cells(const AdjVis& v, const int (*mi)[4],
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          if (base + 32 * u >= ncell) continue;
+          if (base + STRIDE * u >= ncell) continue;
           const double2 t = SCREEN ? cmul_d(sum[u], s[u]) : sum[u];
           double2* dst = region + r * RR + rc[u];
-          atomicAdd(&dst->x, t.x);
-          atomicAdd(&dst->y, t.y);
+          if constexpr (ATOMIC) {
+            atomicAdd(&dst->x, t.x);
+            atomicAdd(&dst->y, t.y);
+          } else {
+            const double2 o = *dst;
+            *dst = make_double2(o.x + t.x, o.y + t.y);
+          }
         }
       }
     }
@@ -209,7 +223,12 @@ adj_tiled_kernel(const __grid_constant__ AdjParams p) {
       region[i] = v;
     }
     __syncthreads();
-    for (int k = warp; k < ch.count; k += kAdjWarps) {
+    // gathers and warp-wide scatters: a warp per visibility; CTA-wide
+    // scatters: every thread on one visibility at a time
+    const bool cta_wide = !gather && p.scatter_cta;
+    const int k0 = cta_wide ? 0 : warp, dk = cta_wide ? 1 : kAdjWarps;
+    const int sub = cta_wide ? int(threadIdx.x) : lane;
+    for (int k = k0; k < ch.count; k += dk) {
       const AdjVis v = adj_vis(p.descs + ch.start + k, p.srefs + ch.start + k);
       const TileDesc* d = p.descs + ch.start + k;
       // Mueller routing and CF sign: gathers use the CF with its imaginary
@@ -239,18 +258,27 @@ adj_tiled_kernel(const __grid_constant__ AdjParams p) {
       // screen, for gathers and scatters (each keeps only its registers)
       if (gather) {
         if (v.screen)
-          vis_cells<N, true, true>(v, mi, im, slice, region, R, RR, p.nrow, lane,
-                                   a, acc);
+          vis_cells<N, true, true, 32, false>(v, mi, im, slice, region, R, RR,
+                                              p.nrow, lane, a, acc);
         else
-          vis_cells<N, true, false>(v, mi, im, slice, region, R, RR, p.nrow,
-                                    lane, a, acc);
+          vis_cells<N, true, false, 32, false>(v, mi, im, slice, region, R, RR,
+                                               p.nrow, lane, a, acc);
+      } else if (cta_wide) {
+        if (v.screen)
+          vis_cells<N, false, true, kAdjThreads, false>(
+              v, mi, im, slice, region, R, RR, p.nrow, sub, a, acc);
+        else
+          vis_cells<N, false, false, kAdjThreads, false>(
+              v, mi, im, slice, region, R, RR, p.nrow, sub, a, acc);
+        // the next visibility may cover the same cells
+        __syncthreads();
       } else {
         if (v.screen)
-          vis_cells<N, false, true>(v, mi, im, slice, region, R, RR, p.nrow,
-                                    lane, a, acc);
+          vis_cells<N, false, true, 32, true>(v, mi, im, slice, region, R, RR,
+                                              p.nrow, lane, a, acc);
         else
-          vis_cells<N, false, false>(v, mi, im, slice, region, R, RR, p.nrow,
-                                     lane, a, acc);
+          vis_cells<N, false, false, 32, true>(v, mi, im, slice, region, R,
+                                               RR, p.nrow, lane, a, acc);
       }
       if (gather) {
 #pragma unroll
@@ -328,6 +356,7 @@ Status linear_op_tiled(hpgb_gridder* g, const void* d_vis, size_t n, int op,
   p.nty = nty;
   p.op = op;
   p.npol = int(g->npol);
+  p.scatter_cta = g->adjoint_scatter_cta;
   p.mt = g->mt;
   p.descs = prep.descs;
   p.srefs = prep.srefs;

@@ -82,9 +82,11 @@ Status launch_batch_n(hpgb_gridder* g0, unsigned npol, const TiledParams& p,
 
 }  // namespace
 
-Status grid_batch_tiled(hpgb_gridder* const* gs, size_t njobs,
-                        void* const* d_vis, const size_t* nvis,
-                        unsigned flags) {
+// One launch over the gridders gs[0..njobs) on gs[0]'s stream, with gs[0]'s
+// buffers; a wait timeout is reported in `status`.
+Status grid_batch_launch(hpgb_gridder* const* gs, size_t njobs,
+                         void* const* d_vis, const size_t* nvis,
+                         unsigned flags, unsigned* status) {
   hpgb_gridder* g0 = gs[0];
   const cudaStream_t st = g0->stream;
   const bool mixed = g0->precision == HPGB_PRECISION_MIXED;
@@ -172,13 +174,72 @@ Status grid_batch_tiled(hpgb_gridder* const* gs, size_t njobs,
   p.chunks = vb.batch_chunks.as<Chunk>();
   p.num_chunks = total_chunks;
   p.rec_stride = int(visdata_size(g0->npol));
-  p.status = vb.counters.as<unsigned>();
+  p.status = status;
   p.wait_limit_ns = g0->wait_limit_ns;
   p.withhold_vis = g0->withhold_vis;
   CUtensorMap unused;
   std::memset(&unused, 0, sizeof(unused));
   if (mixed) return launch_batch_n<true>(g0, g0->npol, p, plan.smem, unused);
   return launch_batch_n<false>(g0, g0->npol, p, plan.smem, unused);
+}
+
+// The gridders are grouped by their widest CF (taps up to 17, 33, 65, more):
+// one launch's plan -- ring depth and tile side -- is sized for its widest
+// CF, so a gridder with narrow CFs in a launch with a wide one would get a
+// shallow ring and small tiles.  Each class takes one launch on the stream
+// of its first gridder, forked from and joined back to gs[0]'s stream, so
+// that the classes' launches overlap where the device has room.
+Status grid_batch_tiled(hpgb_gridder* const* gs, size_t njobs,
+                        void* const* d_vis, const size_t* nvis,
+                        unsigned flags) {
+  auto taps_class = [](const hpgb_gridder* g) {
+    const int t = std::max(g->cf.max_taps_x, g->cf.max_taps_y);
+    return t <= 17 ? 0 : t <= 33 ? 1 : t <= 65 ? 2 : 3;
+  };
+  std::vector<std::vector<size_t>> cls(4);
+  for (size_t j = 0; j < njobs; ++j) cls[taps_class(gs[j])].push_back(j);
+  const cudaStream_t st = gs[0]->stream;
+  unsigned* status = gs[0]->vb.counters.as<unsigned>();
+  int used = 0;
+  for (auto& c : cls) used += !c.empty();
+  if (used <= 1) return grid_batch_launch(gs, njobs, d_vis, nvis, flags, status);
+  cudaEvent_t fork = nullptr;
+  HPGB_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  std::vector<cudaEvent_t> joins;
+  auto cleanup = [&]() {
+    cudaEventDestroy(fork);
+    for (cudaEvent_t e : joins) cudaEventDestroy(e);
+  };
+  Status result = Status::ok();
+  cudaError_t ce = cudaEventRecord(fork, st);
+  for (auto& c : cls) {
+    if (c.empty() || ce != cudaSuccess || !result) continue;
+    std::vector<hpgb_gridder*> sub;
+    std::vector<void*> sv;
+    std::vector<size_t> sn;
+    for (size_t j : c) {
+      sub.push_back(gs[j]);
+      sv.push_back(d_vis[j]);
+      sn.push_back(nvis[j]);
+    }
+    const cudaStream_t cs = sub[0]->stream;
+    if (cs != st) ce = cudaStreamWaitEvent(cs, fork, 0);
+    if (ce != cudaSuccess) break;
+    result = grid_batch_launch(sub.data(), sub.size(), sv.data(), sn.data(),
+                               flags, status);
+    if (cs != st) {
+      cudaEvent_t e = nullptr;
+      ce = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+      if (ce != cudaSuccess) break;
+      joins.push_back(e);
+      ce = cudaEventRecord(e, cs);
+      if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, e, 0);
+    }
+  }
+  cleanup();
+  if (ce != cudaSuccess && result)
+    result = Status::err(HPGB_ERROR_OTHER, cudaGetErrorString(ce));
+  return result;
 }
 
 }  // namespace hpgb

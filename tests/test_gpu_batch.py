@@ -2,9 +2,10 @@
 (hpgb_grid_visibilities_batch), against the oracle per gridder.
 
 The jobs are uneven on purpose: grid sides 96..400 (some rectangular, one
-with two cubes), one to three CF groups each with supports 4..16 at
-oversampling 8, batches of 0..5000 visibilities, two polarizations with a
-diagonal Mueller matrix.  Tolerances as in the single-gridder parity tests:
+with two cubes), one to four CF groups with supports 4..16 (and 24 for
+some, so that the batch spans two support classes, which take a launch
+each on forked streams) at oversampling 8, batches of 0..5000
+visibilities, two polarizations with a diagonal Mueller matrix.  Tolerances as in the single-gridder parity tests:
 FP64 gridding 1e-12; mixed 1e-6; FP64 degrid+grid residuals at least 99%
 bit-exact, and the grid within 1e-12 of the oracle's gridding of the
 device's residuals.
@@ -39,6 +40,9 @@ def make_jobs(seed=1, njobs=9):
         gs = (nx, ny, 2, cubes)
         ngroups = int(rng.integers(1, 4))
         supports = [int(s) for s in rng.integers(4, 17, ngroups)]
+        if j % 4 == 1:  # a wider CF: a second support class, own launch
+            supports.append(24)
+            ngroups += 1
         ext, vals = workloads.separable_cf(
             supports, 8, np.ones(2) + 0.2j * rng.standard_normal(2))
         n = 0 if j == 7 else int(rng.integers(100, 5000))
