@@ -526,14 +526,36 @@ def run_batch(args):
     # each polarization class alone: its batched call against its jobs'
     # own calls
     per_class = {}
+
+    def kernel_ms(cls):
+        """Summed CUDA-event time of the tiled launches recorded since the
+        last call, over the class's gridders (a batched call records its
+        launches on its first gridders: one per support class, which may
+        overlap)."""
+        tot = 0.0
+        for j in cls:
+            ms, n = j["g"].tiled_kernel_time()
+            tot += ms
+        return tot
+
     for k, cls in classes.items():
         one = {k: cls}
+        for j in cls:
+            j["g"].profile_tiled_kernel(True)
+        kernel_ms(cls)
         mb = timed(lambda: batched(one))
+        kb = kernel_ms(cls) / (args.steps + args.warmup)
+        for j in cls:
+            j["g"].profile_tiled_kernel(False)
+        # (the per-job launches' event times are not summed: a launch on
+        # one gridder's stream waits inside its events for the SMs that
+        # the other gridders' launches hold)
         ms = timed(lambda: [j["g"].grid_visibilities(j["dvis"], on_device=True)
                             for j in cls])
         per_class[f"{k}pol"] = {"jobs": len(cls),
                                 "vis": sum(j["nvis"] for j in cls),
-                                "batched_ms": mb, "per_job_ms": ms}
+                                "batched_ms": mb, "per_job_ms": ms,
+                                "batched_kernel_ms_sum": kb}
     for job in jobs:
         job["g"].set_gridding_kernel(abi.KERNEL_TILED)
     ms_single = timed(per_job)

@@ -55,8 +55,6 @@ struct AdjParams {
   const double2* grid_in;  // gathers: model / grid cotangent
   double2* grid_out;       // scatters: accumulated
   const double2* vals_in;  // scatters: [n][npol]
-  int scatter_cta;  // scatters: the CTA on one visibility at a time (1) or a
-                    // warp per visibility with shared-memory atomics (0)
   double2* vals_out;       // gathers: [n][npol]
 };
 
@@ -97,11 +95,12 @@ __device__ __forceinline__ AdjVis adj_vis(const TileDesc* d, const SliceRef* s) 
 // HBM reads in flight -- the slices stream from HBM once, nothing to
 // reuse).  GATHER: acc += CF' * (region * screen) per polarization;
 // otherwise region += screen * sum_q CF' * a[q] with shared-memory atomics.
-// STRIDE threads share the visibility's cells (a warp, or the whole CTA);
-// ATOMIC: scatters add with shared-memory atomics (a warp per visibility,
-// footprints of concurrent visibilities may overlap) or with plain
-// read-modify-writes (the CTA on one visibility at a time: no two threads
-// touch a cell).
+// STRIDE threads share the visibility's cells (a warp); ATOMIC: scatters
+// add with shared-memory atomics (warps take different visibilities, whose
+// footprints may overlap).  A CTA-wide scatter (every thread on one
+// visibility, plain read-modify-writes, a barrier between visibilities) was
+// measured 1.8x slower at 10M visibilities: each visibility's CF loads then
+// wait in turn.
 template <int N, bool GATHER, bool SCREEN, int STRIDE, bool ATOMIC>
 __device__ __forceinline__ void vis_cells(const AdjVis& v, const int (*mi)[4],
                                           double im, const float2* slice,
@@ -223,12 +222,7 @@ adj_tiled_kernel(const __grid_constant__ AdjParams p) {
       region[i] = v;
     }
     __syncthreads();
-    // gathers and warp-wide scatters: a warp per visibility; CTA-wide
-    // scatters: every thread on one visibility at a time
-    const bool cta_wide = !gather && p.scatter_cta;
-    const int k0 = cta_wide ? 0 : warp, dk = cta_wide ? 1 : kAdjWarps;
-    const int sub = cta_wide ? int(threadIdx.x) : lane;
-    for (int k = k0; k < ch.count; k += dk) {
+    for (int k = warp; k < ch.count; k += kAdjWarps) {
       const AdjVis v = adj_vis(p.descs + ch.start + k, p.srefs + ch.start + k);
       const TileDesc* d = p.descs + ch.start + k;
       // Mueller routing and CF sign: gathers use the CF with its imaginary
@@ -263,15 +257,6 @@ adj_tiled_kernel(const __grid_constant__ AdjParams p) {
         else
           vis_cells<N, true, false, 32, false>(v, mi, im, slice, region, R, RR,
                                                p.nrow, lane, a, acc);
-      } else if (cta_wide) {
-        if (v.screen)
-          vis_cells<N, false, true, kAdjThreads, false>(
-              v, mi, im, slice, region, R, RR, p.nrow, sub, a, acc);
-        else
-          vis_cells<N, false, false, kAdjThreads, false>(
-              v, mi, im, slice, region, R, RR, p.nrow, sub, a, acc);
-        // the next visibility may cover the same cells
-        __syncthreads();
       } else {
         if (v.screen)
           vis_cells<N, false, true, 32, true>(v, mi, im, slice, region, R, RR,
@@ -356,7 +341,6 @@ Status linear_op_tiled(hpgb_gridder* g, const void* d_vis, size_t n, int op,
   p.nty = nty;
   p.op = op;
   p.npol = int(g->npol);
-  p.scatter_cta = g->adjoint_scatter_cta;
   p.mt = g->mt;
   p.descs = prep.descs;
   p.srefs = prep.srefs;

@@ -10,8 +10,10 @@
 // tile-pass lists into one work list, each pass tagged with its gridder,
 // and the tiled kernel reads each pass's grid, weights, CF, records, tile
 // geometry and model tensor map from a job table in device memory
-// (BatchJob).  All of it runs on the first gridder's stream; the others'
-// streams are ordered before and after it.  The gridders must share the
+// (BatchJob).  The sorts run on the gridders' own streams, forked from the
+// first gridder's stream and joined back before the launch, which runs
+// there; the others' streams are ordered before and after the whole call.
+// The gridders must share the
 // number of polarizations and grid rows, the Mueller tables, the arithmetic
 // form and (when degridding) whether a model is set.
 
@@ -90,13 +92,16 @@ Status grid_batch_launch(hpgb_gridder* const* gs, size_t njobs,
   hpgb_gridder* g0 = gs[0];
   const cudaStream_t st = g0->stream;
   const bool mixed = g0->precision == HPGB_PRECISION_MIXED;
-  BatchShape shape{0, 0};
+  BatchShape shape;
   size_t total = 0;
   for (size_t j = 0; j < njobs; ++j) {
-    for (const CFGroup& G : gs[j]->cf.groups)
+    const hpgb_gridder* g = gs[j];
+    for (const CFGroup& G : g->cf.groups)
       shape.max_plane_bytes = std::max(shape.max_plane_bytes, G.plane_stride * 8);
-    shape.max_taps = std::max(
-        shape.max_taps, std::max(gs[j]->cf.max_taps_x, gs[j]->cf.max_taps_y));
+    const int taps = std::max(g->cf.max_taps_x, g->cf.max_taps_y);
+    shape.max_taps = std::max(shape.max_taps, taps);
+    shape.jobs.push_back({(long long)g->grid_size[0], (long long)g->grid_size[1],
+                          (long long)g->grid_size[3], taps, (long long)nvis[j]});
     total += nvis[j];
   }
   if (total == 0) return Status::ok();
@@ -123,10 +128,28 @@ Status grid_batch_launch(hpgb_gridder* const* gs, size_t njobs,
                            "gridder " + std::to_string(j) +
                                ": model row pitch not a 16-byte multiple "
                                "(odd grid width in the mixed form)");
+  // Each gridder's tile sort (and FP32 model copy) runs on the gridder's own
+  // stream, forked from st and joined back before the launch, so that the
+  // gridders' short preparation kernels overlap one another instead of
+  // queueing one after another on st.  Their buffers are the gridder's own.
+  cudaEvent_t fork = nullptr;
+  HPGB_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  std::vector<cudaEvent_t> joins;
+  struct Release {
+    cudaEvent_t& f;
+    std::vector<cudaEvent_t>& j;
+    ~Release() {
+      cudaEventDestroy(f);
+      for (cudaEvent_t e : j) cudaEventDestroy(e);
+    }
+  } release{fork, joins};
+  HPGB_CUDA_TRY(cudaEventRecord(fork, st));
   for (size_t j = 0; j < njobs; ++j) {
     hpgb_gridder* g = gs[j];
     BatchJob& b = jobs[j];
     std::memset(&b, 0, sizeof(b));
+    const cudaStream_t js = g->stream;
+    if (js != st) HPGB_CUDA_TRY(cudaStreamWaitEvent(js, fork, 0));
     const int taps = std::max(g->cf.max_taps_x, g->cf.max_taps_y);
     // the largest tile this gridder's CF allows in the launch's region
     b.T = R - taps + 1;
@@ -141,7 +164,7 @@ Status grid_batch_launch(hpgb_gridder* const* gs, size_t njobs,
     if (nvis[j] > 0) {
       TilePrep prep;
       HPGB_TRY(prepare_tiles(g, d_vis[j], nvis[j], b.T, b.ntx, b.nty, plan.K,
-                             &prep, st));
+                             &prep, js));
       b.descs = prep.descs;
       b.srefs = prep.srefs;
       srcs[j] = ChunkSrc{prep.chunks, prep.num_chunks};
@@ -150,9 +173,16 @@ Status grid_batch_launch(hpgb_gridder* const* gs, size_t njobs,
       // no passes: point at a zero count
       srcs[j] = ChunkSrc{nullptr, g->vb.counters.as<unsigned>() + 3};
       HPGB_CUDA_TRY(cudaMemsetAsync(g->vb.counters.as<unsigned>() + 3, 0,
-                                    sizeof(unsigned), st));
+                                    sizeof(unsigned), js));
     }
-    if (model) HPGB_TRY(encode_model_map(g, mixed, R, &b.model_map, st));
+    if (model) HPGB_TRY(encode_model_map(g, mixed, R, &b.model_map, js));
+    if (js != st) {
+      cudaEvent_t e = nullptr;
+      HPGB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      joins.push_back(e);
+      HPGB_CUDA_TRY(cudaEventRecord(e, js));
+      HPGB_CUDA_TRY(cudaStreamWaitEvent(st, e, 0));
+    }
   }
   // job table and the combined work list, in g0's buffers
   VisBuffers& vb = g0->vb;

@@ -402,10 +402,20 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
       R = tp.tile_side;
     }
     if (R - taps + 1 < 4) continue;
-    if (!fixed && m > m_lo && !batch) {
-      const size_t T = size_t(R - taps + 1);
-      const size_t ntiles = ((g->grid_size[0] + T - 1) / T) *
-                            ((g->grid_size[1] + T - 1) / T) * g->grid_size[3];
+    if (!fixed && m > m_lo) {
+      // tiles of the batch (of every gridder of a batched launch, each
+      // with the largest tile its own CF allows in the region)
+      auto tiles = [R](size_t nx, size_t ny, size_t ncube, int t) {
+        const size_t T = size_t(R - t + 1);
+        return ((nx + T - 1) / T) * ((ny + T - 1) / T) * ncube;
+      };
+      size_t ntiles = 0;
+      if (batch) {
+        for (const BatchShape::Job& j : batch->jobs)
+          if (j.nvis > 0) ntiles += tiles(j.nx, j.ny, j.ncube, int(j.taps));
+      } else {
+        ntiles = tiles(g->grid_size[0], g->grid_size[1], g->grid_size[3], taps);
+      }
       if (nvis < kMinVisPerTile * ntiles) continue;
     }
     pl.ring_bytes = rb;

@@ -98,9 +98,6 @@ struct hpgb_gridder {
   // (a visibility whose copies CTA 0 never issues; -1: none)
   unsigned long long wait_limit_ns = 500000000ull;
   long long withhold_vis = -1;
-  // tiled scatter operators (D^H, G): the CTA on one visibility at a time
-  // (1) or a warp per visibility with shared-memory atomics (0)
-  int adjoint_scatter_cta = 1;
 
   hpgb::CFRegion cf;
   hpgb::VisBuffers vb;

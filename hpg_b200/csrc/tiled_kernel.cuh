@@ -9,6 +9,7 @@
 
 #include <string>
 #include <type_traits>
+#include <vector>
 
 #include "gridder.cuh"
 #include "ptx.cuh"
@@ -101,9 +102,12 @@ struct TiledParams {
   long long withhold_vis;
 };
 
-// single fields of a tile pass's gridder, read where they are used (the
-// launch parameters live in the constant bank; holding them in registers
-// across a pass would only add register pressure)
+// single fields of a tile pass's gridder: from the launch parameters (the
+// constant bank), or in a batched launch from the job table in global
+// memory.  The consumer roles read them where they are used, once per pass
+// (holding them across a pass would add register pressure to the cell
+// loops); the producer warps, which need the descriptor and CF bases for
+// every visibility, read those once per pass into registers.
 #define HPGB_JOB(BATCH, p, j, field) ((BATCH) ? (p).jobs[j].field : (p).field)
 
 struct SmemLayout {
@@ -576,9 +580,12 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       run_dst[u] = p.run_dst[row][u];
     }
     const bool cf_needed = exchange || p.do_grid;
-    // the copies of one visibility into slot s (one thread)
-    auto issue = [&](int job, int s, int roff, long long off, int pstride,
-                     int dindex, uint32_t qv) {
+    // the copies of one visibility into slot s (one thread); jdescs, jcf:
+    // the descriptors and CF of the pass's gridder (read from the job table
+    // once per pass in a batched launch)
+    auto issue = [&](const TileDesc* jdescs, const float2* jcf, int s,
+                     int roff, long long off, int pstride, int dindex,
+                     uint32_t qv) {
       // test hook: CTA 0 never issues the copies of one visibility, so that
       // the waits for them run out (the slot's phase never completes)
       if (blockIdx.x == 0 && (long long)qv == p.withhold_vis) return;
@@ -586,12 +593,11 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       const uint32_t need = cf_needed ? uint32_t(nplanes) * pbytes : 0u;
       ring_off[s] = roff;
       ptx::mbar_expect_tx(&full[s], uint32_t(sizeof(TileDesc)) + need);
-      ptx::bulk_g2s(&descs[s], &HPGB_JOB(BATCH, p, job, descs)[dindex],
-                    uint32_t(sizeof(TileDesc)),
+      ptx::bulk_g2s(&descs[s], &jdescs[dindex], uint32_t(sizeof(TileDesc)),
                     &full[s]);
       if (cf_needed) {
         unsigned char* dst = ring + roff;
-        const float2* slice = HPGB_JOB(BATCH, p, job, cf) + off;
+        const float2* slice = jcf + off;
 #pragma unroll
         for (int u = 0; u < kMaxRuns; ++u)
           if (u < nruns)
@@ -610,6 +616,8 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       for (unsigned c = cid; c < nchunks; c += ncl) {
         const int count = p.chunks[c].count;
         const int cjob = BATCH ? p.chunks[c].pad : 0;
+        const TileDesc* jdescs = HPGB_JOB(BATCH, p, cjob, descs);
+        const float2* jcf = HPGB_JOB(BATCH, p, cjob, cf);
 
         for (int k = int((h + kProducers - q % kProducers) % kProducers);
              k < count; k += kProducers) {
@@ -617,8 +625,8 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           const int s = int(qq % uint32_t(kSlots));
           ok &= ptx::mbar_wait(&req[s], (qq / kSlots) & 1, abort);
           if (lane == 0 && !*abort)
-            issue(cjob, s, req_off[s], req_src[s], req_pst[s], req_desc[s],
-                  qq);
+            issue(jdescs, jcf, s, req_off[s], req_src[s], req_pst[s],
+                  req_desc[s], qq);
           __syncwarp();
         }
         q += uint32_t(count);
@@ -630,12 +638,14 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       unsigned long long tail = 0;      // ring bytes released (monotonic)
       for (unsigned c = cid; c < nchunks; c += ncl) {
         const Chunk ch = p.chunks[c];
+        const TileDesc* jdescs = HPGB_JOB(BATCH, p, ch.pad, descs);
+        const float2* jcf = HPGB_JOB(BATCH, p, ch.pad, cf);
+        const SliceRef* jsrefs = HPGB_JOB(BATCH, p, ch.pad, srefs);
         SliceRef cur{};
         for (int k = 0; k < ch.count; ++k, ++q) {
           if ((k & 31) == 0) {
             cur = SliceRef{};
-            if (k + lane < ch.count)
-              cur = HPGB_JOB(BATCH, p, ch.pad, srefs)[ch.start + k + lane];
+            if (k + lane < ch.count) cur = jsrefs[ch.start + k + lane];
           }
           const int kk = k & 31;
           const long long off = __shfl_sync(0xffffffffu, cur.off, kk);
@@ -674,7 +684,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           if (lane == 0 && !*abort) {
             slot_end[s] = head + need;
             if (q % kProducers == 0) {
-              issue(ch.pad, s, int(pos), off, pstride, ch.start + k, q);
+              issue(jdescs, jcf, s, int(pos), off, pstride, ch.start + k, q);
             } else {
               req_off[s] = int(pos);
               req_src[s] = off;
@@ -693,7 +703,9 @@ tiled_kernel(const __grid_constant__ TiledParams p,
     // ---------------- consumer roles ----------------
     // degridding warps [0, kDG), exchange warps [kXBase, kGRBase), gridding
     // warps [kGRBase, kGRBase + kGR).  Roles hand visibilities to each other
-    // through mbarriers; all of them meet at chunk boundaries.
+    // through mbarriers and never wait for one another at chunk boundaries:
+    // the degridding warps meet there among themselves (model tile), the
+    // gridding warps among themselves (zeroing and flush of their tiles).
     uint32_t q = 0;
     uint32_t model_phase = 0;
     // the model tile of this cluster's chunk cc, copied by one thread.  FP64
@@ -733,24 +745,19 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       const int ty = (tile / jntx) % jnty;
       const int cube = tile / (jntx * jnty);
       const int x0 = tx * jT, y0 = ty * jT;
-      ptx::named_sync(1, kConsumers);
-      if (!kEarlyModel && exchange && tid == 0 && !*abort) load_model(c);
-      if (p.do_grid)
-        for (int i = tid; i < RR * kTiles; i += kConsumers) {
-          GT z;
-          z.x = 0;
-          z.y = 0;
-          gtile[i] = z;
-        }
-      if (exchange) {
-        ok &= ptx::mbar_wait(model_bar, model_phase, abort);
-        model_phase ^= 1;
-      }
-      ptx::named_sync(1, kConsumers);
-      double wchunk = 0.0;
 
       if (warp < kDG) {
         // -------- degridding warps --------
+        // the chunk's model tile: mixed form, loaded here once every
+        // degridding warp (its only readers) is done with the previous one
+        if constexpr (!kEarlyModel) {
+          ptx::named_sync(4, kDG * 32);
+          if (exchange && tid == 0 && !*abort) load_model(c);
+        }
+        if (exchange) {
+          ok &= ptx::mbar_wait(model_bar, model_phase, abort);
+          model_phase ^= 1;
+        }
         const int grp = warp / kDGPer;
         for (int k = 0; k < ch.count; ++k, ++q) {
           const int s = int(q % uint32_t(kSlots));
@@ -845,6 +852,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         // after this warp finished q: the buffer is never overwritten while
         // it is read.
         const int xw = warp - kXBase;
+        double wchunk = 0.0;  // this warp's share of the row's weight sum
         for (int k = 0; k < ch.count; ++k, ++q) {
           if ((q & 1) != uint32_t(xw)) continue;
           {
@@ -943,6 +951,10 @@ tiled_kernel(const __grid_constant__ TiledParams p,
             __syncwarp();
           }
         }
+        if (lane == 0 && p.do_grid && p.update_weights && wchunk != 0.0 &&
+            !*abort)
+          atomicAdd(HPGB_JOB(BATCH, p, job, weights) + size_t(cube) * p.nrow + row,
+                    wchunk);
       } else {
         // -------- gridding warps --------
         // The gridding warps form kGT groups: group g takes the
@@ -954,6 +966,22 @@ tiled_kernel(const __grid_constant__ TiledParams p,
         const int gw = warp - kGRBase;
         constexpr int gper = kGR / kGT;  // warps per group
         const int grp = gw / gper;
+        // Thread gt of the gridding warps zeroes, and after the chunk
+        // flushes, the tile cells gt, gt + kGR * 32, ... of every tile; a
+        // barrier of the gridding warps alone (id 5) separates the zeroing
+        // from the chunk's first additions and the last additions from the
+        // flush, so the other roles run on into the next chunk meanwhile.
+        const int gt = tid - kGRBase * 32;
+        if (p.do_grid)
+          for (int i = gt; i < RR; i += kGR * 32)
+#pragma unroll
+            for (int t = 0; t < kTiles; ++t) {
+              GT z;
+              z.x = 0;
+              z.y = 0;
+              gtile[t * RR + i] = z;
+            }
+        ptx::named_sync(5, kGR * 32);
         const uint32_t mytile =
             ptx::smem(gtile) + uint32_t(grp * RR) * uint32_t(sizeof(GT));
         // compensated tiles: the low parts of the groups' tiles follow their
@@ -1007,36 +1035,32 @@ tiled_kernel(const __grid_constant__ TiledParams p,
           __syncwarp();
           if (lane == 0) ptx::mbar_arrive(&empty[s]);
         }
-      }
-      ptx::named_sync(1, kConsumers);
-      if (p.do_grid && !*abort) {
-        const int jnx = HPGB_JOB(BATCH, p, job, nx);
-        const int jny = HPGB_JOB(BATCH, p, job, ny);
-        double2* plane = HPGB_JOB(BATCH, p, job, grid) +
-                         size_t(cube * p.nrow + row) * jny * jnx;
-        for (int i = tid; i < RR; i += kConsumers) {
-          const int gx = x0 + i % R, gy = y0 + i / R;
-          if (gx < jnx && gy < jny) {
-            // the gridding groups' tiles (with their low parts), summed in
-            // FP64
-            double vx = 0.0, vy = 0.0;
+        ptx::named_sync(5, kGR * 32);
+        if (p.do_grid && !*abort) {
+          const int jnx = HPGB_JOB(BATCH, p, job, nx);
+          const int jny = HPGB_JOB(BATCH, p, job, ny);
+          double2* plane = HPGB_JOB(BATCH, p, job, grid) +
+                           size_t(cube * p.nrow + row) * jny * jnx;
+          for (int i = gt; i < RR; i += kGR * 32) {
+            const int gx = x0 + i % R, gy = y0 + i / R;
+            if (gx < jnx && gy < jny) {
+              // the gridding groups' tiles (with their low parts), summed in
+              // FP64
+              double vx = 0.0, vy = 0.0;
 #pragma unroll
-            for (int t = 0; t < kTiles; ++t) {
-              const GT v = gtile[t * RR + i];
-              vx += double(v.x);
-              vy += double(v.y);
-            }
-            if (vx != 0 || vy != 0) {
-              double2* dst = plane + size_t(gy) * jnx + gx;
-              atomicAdd(&dst->x, vx);
-              atomicAdd(&dst->y, vy);
+              for (int t = 0; t < kTiles; ++t) {
+                const GT v = gtile[t * RR + i];
+                vx += double(v.x);
+                vy += double(v.y);
+              }
+              if (vx != 0 || vy != 0) {
+                double2* dst = plane + size_t(gy) * jnx + gx;
+                atomicAdd(&dst->x, vx);
+                atomicAdd(&dst->y, vy);
+              }
             }
           }
         }
-        if (warp >= kXBase && warp < kGRBase && lane == 0 && p.update_weights &&
-            wchunk != 0.0)
-          atomicAdd(HPGB_JOB(BATCH, p, job, weights) + size_t(cube) * p.nrow + row,
-                    wchunk);
       }
     }
   }
@@ -1063,11 +1087,16 @@ tiled_kernel(const __grid_constant__ TiledParams p,
 // ---------------------------------------------------------------------------
 // host side shared by grid_tiled.cu and grid_batch.cu
 
-// the CF shape of a batched launch: the largest plane and support over its
-// gridders
+// the shape of a batched launch: the largest CF plane and support over its
+// gridders, and per gridder its grid (width, height, cubes), widest CF
+// (taps) and batch size, from which the plan counts the launch's tiles
 struct BatchShape {
-  int max_plane_bytes;
-  int max_taps;
+  struct Job {
+    long long nx, ny, ncube, taps, nvis;
+  };
+  int max_plane_bytes = 0;
+  int max_taps = 0;
+  std::vector<Job> jobs;
 };
 
 struct Plan {
