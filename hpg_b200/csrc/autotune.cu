@@ -207,15 +207,22 @@ Status autotune_tiled(hpgb_gridder* g, const void* vis, size_t n,
   // 1. ring depth
   for (int ring = 2; st && ring <= 8; ++ring) st = trial(Trial{ring, 0, 0});
   if (!st || best_ms == std::numeric_limits<float>::max()) return finish(st);
-  // 2. tile side below the largest that fits at that depth
-  g->tplan.ring_parts = best.ring_parts;
-  g->tplan.tile_side = 0;
-  int side = 0;
-  if (tiled_plan_side(g, flags, n, &side) && side > 0) {
+  // 2. tile sides below the largest that fits at that depth and one part
+  // shallower: a smaller side gives the bytes it frees to the ring, so
+  // these trials fill in ring sizes between whole parts (more visibilities
+  // in flight against more, shorter tile passes)
+  {
     const int taps = std::max(g->cf.max_taps_x, g->cf.max_taps_y);
-    for (int d : {8, 16})
-      if (st && side - d - taps + 1 >= 4)
-        st = trial(Trial{best.ring_parts, 0, side - d});
+    const int deepest = best.ring_parts;
+    for (int ring = deepest; st && ring >= std::max(2, deepest - 1); --ring) {
+      g->tplan.ring_parts = ring;
+      g->tplan.tile_side = 0;
+      int side = 0;
+      if (!tiled_plan_side(g, flags, n, &side) || side <= 0) continue;
+      for (int d : {0, 4, 8, 12, 16})
+        if (st && side - d - taps + 1 >= 4)
+          st = trial(Trial{ring, 0, side - d});
+    }
   }
   // 3. tile-pass length
   const bool mixed = g->precision == HPGB_PRECISION_MIXED;

@@ -418,7 +418,11 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
       }
       if (nvis < kMinVisPerTile * ntiles) continue;
     }
-    pl.ring_bytes = rb;
+    // the ring takes every whole KB the tiles leave (the ring's bytes, not
+    // its part count, set how many visibilities are in flight; a tile side
+    // below the largest thus deepens the ring)
+    const int spare = left - per_cell * R * R;
+    pl.ring_bytes = rb + (spare >= 1024 ? spare / 1024 * 1024 : 0);
     pl.R = R;
     break;
   }

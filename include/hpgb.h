@@ -377,7 +377,9 @@ HPGB_API int hpgb_set_tiled_plan(hpgb_gridder* gridder, int ring_parts,
  *  tile_side      even, at most 128: side R of the shared-memory uv tile in
  *                 cells (the largest that fits the ring's leftover shared
  *                 memory when 0); a side the ring leaves no room for makes
- *                 the plan not fit;
+ *                 the plan not fit; the CF ring takes every whole KB the
+ *                 tiles leave (at least ring_parts parts), so a smaller
+ *                 side deepens the ring;
  *  compensated    mixed form only: 1: plain FP32 grid tiles; 2: FP32
  *                 high/low tile pairs updated by two-sum, so that the tile
  *                 adds no accumulation error however long the pass (the
