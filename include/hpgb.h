@@ -446,9 +446,10 @@ HPGB_API int hpgb_last_gridding_kernel(const hpgb_gridder* gridder,
 
 /* Autotuner of the tiled kernel, no counterpart in the reference: runs the
  * batch (as hpgb_grid_visibilities would with these flags) three times per
- * candidate plan -- CF ring depths 2..8, then uv tile sides 8 and 16 cells
- * below the largest that fits at the fastest depth, then tile-pass lengths
- * -- ranks the candidates by their median CUDA-event time (a launch that
+ * candidate plan -- CF ring depths 2..8, then uv tile sides 0, 4, 8, 12 and
+ * 16 cells below the largest that fits at the fastest depth and at one part
+ * less (the ring takes the bytes a smaller side frees), then tile-pass
+ * lengths -- ranks the candidates by their median CUDA-event time (a launch that
  * reported a device wait timeout does not count), restores the grid and
  * weights on every exit path, and keeps the fastest plan for the gridder's
  * later calls (readable with hpgb_get_tiled_plan), returning its ring depth
@@ -456,7 +457,7 @@ HPGB_API int hpgb_last_gridding_kernel(const hpgb_gridder* gridder,
  * are cached in the process per workload (grid shape, polarizations,
  * Mueller tables, CF group shapes, precision, compensation, flags, model,
  * log2 of the batch size): a later call with the same workload applies the
- * cached plan at once.  Synchronous; costs about forty runs of the batch
+ * cached plan at once.  Synchronous; costs about sixty runs of the batch
  * the first time: tune on a representative batch once, then grid. */
 HPGB_API int hpgb_autotune_tiled(hpgb_gridder* gridder, const void* visibilities,
                                  size_t num_visibilities,
