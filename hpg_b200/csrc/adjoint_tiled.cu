@@ -16,6 +16,9 @@
 //     into the shared region with FP64 shared-memory atomics (warps take
 //     different visibilities, whose footprints may overlap); the pass ends
 //     with one FP64 global atomic per region cell and row.
+// The region is held as two planes, real and imaginary parts, so that a
+// warp's atomics on consecutive cells touch consecutive 8-byte words (half
+// the shared-memory wavefronts of interleaved complex values).
 // Each CF value crosses HBM once per visibility, each grid cell once per
 // pass (plus the region's halo of taps - 1 cells).  Arithmetic and signs are
 // those of the per-visibility kernels in adjoint.cu, so both satisfy the
@@ -104,8 +107,8 @@ __device__ __forceinline__ AdjVis adj_vis(const TileDesc* d, const SliceRef* s) 
 template <int N, bool GATHER, bool SCREEN, int STRIDE, bool ATOMIC>
 __device__ __forceinline__ void vis_cells(const AdjVis& v, const int (*mi)[4],
                                           double im, const float2* slice,
-                                          double2* region, int R, int RR,
-                                          int nrow, int lane,
+                                          double* re_plane, double* im_plane,
+                                          int R, int RR, int nrow, int lane,
                                           const double2 (&a)[N],
                                           double (&acc)[2 * N]) {
   constexpr int U = (!SCREEN && N <= 2) ? 8 : 4;
@@ -131,7 +134,8 @@ __device__ __forceinline__ void vis_cells(const AdjVis& v, const int (*mi)[4],
         double2 gs[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          gs[u] = region[r * RR + rc[u]];
+          gs[u] = make_double2(re_plane[r * RR + rc[u]],
+                               im_plane[r * RR + rc[u]]);
           if constexpr (SCREEN) gs[u] = cmul_d(gs[u], s[u]);
         }
 #pragma unroll
@@ -178,13 +182,14 @@ __device__ __forceinline__ void vis_cells(const AdjVis& v, const int (*mi)[4],
         for (int u = 0; u < U; ++u) {
           if (base + STRIDE * u >= ncell) continue;
           const double2 t = SCREEN ? cmul_d(sum[u], s[u]) : sum[u];
-          double2* dst = region + r * RR + rc[u];
+          double* dre = re_plane + r * RR + rc[u];
+          double* dim = im_plane + r * RR + rc[u];
           if constexpr (ATOMIC) {
-            atomicAdd(&dst->x, t.x);
-            atomicAdd(&dst->y, t.y);
+            atomicAdd(dre, t.x);
+            atomicAdd(dim, t.y);
           } else {
-            const double2 o = *dst;
-            *dst = make_double2(o.x + t.x, o.y + t.y);
+            *dre += t.x;
+            *dim += t.y;
           }
         }
       }
@@ -195,12 +200,15 @@ __device__ __forceinline__ void vis_cells(const AdjVis& v, const int (*mi)[4],
 template <int N>
 __global__ void __launch_bounds__(kAdjThreads, 1)
 adj_tiled_kernel(const __grid_constant__ AdjParams p) {
-  extern __shared__ __align__(16) double2 region[];  // [nrow][R][R]
+  // [nrow][R][R] real parts, then [nrow][R][R] imaginary parts
+  extern __shared__ __align__(16) double region[];
   __shared__ unsigned cur_chunk;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool gather = p.op == 0 || p.op == 3;
   const bool degrid_set = p.op == 0 || p.op == 1;
   const int R = p.R, RR = R * R;
+  double* const re_plane = region;
+  double* const im_plane = region + size_t(p.nrow) * RR;
   const unsigned nchunks = *p.num_chunks;
   for (;;) {
     __syncthreads();  // the previous pass is done with the region
@@ -219,7 +227,8 @@ adj_tiled_kernel(const __grid_constant__ AdjParams p) {
       double2 v = make_double2(0.0, 0.0);
       if (gather && gx < p.nx && gy < p.ny)
         v = p.grid_in[(size_t(cube * p.nrow + r) * p.ny + gy) * p.nx + gx];
-      region[i] = v;
+      re_plane[i] = v.x;
+      im_plane[i] = v.y;
     }
     __syncthreads();
     for (int k = warp; k < ch.count; k += kAdjWarps) {
@@ -252,18 +261,22 @@ adj_tiled_kernel(const __grid_constant__ AdjParams p) {
       // screen, for gathers and scatters (each keeps only its registers)
       if (gather) {
         if (v.screen)
-          vis_cells<N, true, true, 32, false>(v, mi, im, slice, region, R, RR,
-                                              p.nrow, lane, a, acc);
+          vis_cells<N, true, true, 32, false>(v, mi, im, slice, re_plane,
+                                              im_plane, R, RR, p.nrow, lane,
+                                              a, acc);
         else
-          vis_cells<N, true, false, 32, false>(v, mi, im, slice, region, R, RR,
-                                               p.nrow, lane, a, acc);
+          vis_cells<N, true, false, 32, false>(v, mi, im, slice, re_plane,
+                                               im_plane, R, RR, p.nrow, lane,
+                                               a, acc);
       } else {
         if (v.screen)
-          vis_cells<N, false, true, 32, true>(v, mi, im, slice, region, R, RR,
-                                              p.nrow, lane, a, acc);
+          vis_cells<N, false, true, 32, true>(v, mi, im, slice, re_plane,
+                                              im_plane, R, RR, p.nrow, lane,
+                                              a, acc);
         else
-          vis_cells<N, false, false, 32, true>(v, mi, im, slice, region, R,
-                                               RR, p.nrow, lane, a, acc);
+          vis_cells<N, false, false, 32, true>(v, mi, im, slice, re_plane,
+                                               im_plane, R, RR, p.nrow, lane,
+                                               a, acc);
       }
       if (gather) {
 #pragma unroll
@@ -290,7 +303,7 @@ adj_tiled_kernel(const __grid_constant__ AdjParams p) {
       for (int i = threadIdx.x; i < RR * p.nrow; i += kAdjThreads) {
         const int r = i / RR, j = i - r * RR;
         const int gx = x0 + j % R, gy = y0 + j / R;
-        const double2 v = region[i];
+        const double2 v = make_double2(re_plane[i], im_plane[i]);
         if (gx < p.nx && gy < p.ny && (v.x != 0.0 || v.y != 0.0)) {
           double2* dst =
               p.grid_out + (size_t(cube * p.nrow + r) * p.ny + gy) * p.nx + gx;
