@@ -41,13 +41,16 @@
 //                           shared-memory grid tile (mixed form: two groups
 //                           of 4 take alternate visibilities, each with a
 //                           tile of its own);
-//                         - at the end of a chunk the tile (the sum of the
-//                           groups' tiles, with their low parts in the
-//                           compensated form) is added to the FP64 grid
-//                           with two scalar FP64 reductions per cell (an
-//                           atomicAdd whose result is unused compiles to a
-//                           reduction; PTX has no vector FP64 reduction),
-//                           and the row's weight sum to the weights.  The
+//                         - at the end of a chunk the gridding warps add
+//                           the tile (the sum of the groups' tiles, with
+//                           their low parts in the compensated form) to the
+//                           FP64 grid and zero it, between barriers of
+//                           their own, while the other roles run on into
+//                           the next chunk: two scalar FP64 reductions per
+//                           cell (an atomicAdd whose result is unused
+//                           compiles to a reduction; PTX has no vector FP64
+//                           reduction); the exchange warps add the row's
+//                           weight sum to the weights.  The
 //                           reductions take under 3% of the L2's reduction
 //                           throughput (lts__t_sectors_srcunit_tex_op_red in
 //                           the kernel's ncu capture): one per tile cell per

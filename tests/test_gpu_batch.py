@@ -5,7 +5,8 @@ The jobs are uneven on purpose: grid sides 96..400 (some rectangular, one
 with two cubes), one to four CF groups with supports 4..16 (and 24 for
 some, so that the batch spans two support classes, which take a launch
 each on forked streams) at oversampling 8, batches of 0..5000
-visibilities, two polarizations with a diagonal Mueller matrix.  Tolerances as in the single-gridder parity tests:
+visibilities, two polarizations with a diagonal Mueller matrix; a second
+set reaches support 64 (three support classes).  Tolerances as in the single-gridder parity tests:
 FP64 gridding 1e-12; mixed 1e-6; FP64 degrid+grid residuals at least 99%
 bit-exact, and the grid within 1e-12 of the oracle's gridding of the
 device's residuals.
@@ -116,6 +117,61 @@ def test_batch_matches_oracle(gpu, oracle_lib, precision, comp, degrid):
             if degrid:
                 assert rel_norm(res["vis"], exp["vis"]) <= 1e-6
             assert rel_norm(grid, o.grid) <= 1e-6, k
+    for g in gs:
+        g.close()
+
+
+def make_wide_jobs(seed=5):
+    """Gridders whose widest CFs reach support 64 (65 taps: the launch of
+    that support class takes a two- or three-part CF ring) beside ones
+    whose widest are 32 and 16 (three support classes, three launches),
+    two polarizations, diagonal Mueller."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for supports in ([64], [8, 64], [32], [16, 32], [64, 32, 8], [8, 16]):
+        nx = int(rng.integers(80, 160)) * 2
+        gs = (nx, nx, 2, 1)
+        ext, vals = workloads.separable_cf(
+            supports, 8, np.ones(2) + 0.2j * rng.standard_normal(2))
+        n = int(rng.integers(300, 1500))
+        vis = workloads.visibilities(n, 2, gs, (0.05, 0.05), 1.4e9, rng,
+                                     disk=0.3, w_frac=0.2,
+                                     ngroups=len(supports), grad=0.2)
+        model = (rng.standard_normal((1, 2, nx, nx)) +
+                 1j * rng.standard_normal((1, 2, nx, nx)))
+        jobs.append(dict(grid_size=gs, cf_extents=ext, cf_values=vals,
+                         vis=vis, model=model))
+    return jobs
+
+
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED],
+                         ids=["fp64", "mixed"])
+def test_batch_wide_supports(gpu, oracle_lib, precision):
+    """The batched launches at supports up to 64 (three support classes:
+    shallow rings and large tiles for the widest) against the oracle per
+    gridder, degrid+grid."""
+    O = oracle_lib
+    jobs = make_wide_jobs()
+    gs = gridders_for(jobs, precision, 0, True)
+    futs = hpg_b200.grid_visibilities_batch(
+        gs, [j["vis"] for j in jobs], do_degrid=True,
+        return_visibilities=True)
+    gs[0].fence()
+    for k, (job, g, fut) in enumerate(zip(jobs, gs, futs)):
+        o = oracle_for(O, job, True)
+        exp = o.grid_visibilities(job["vis"], do_degrid=True, return_vis=True)
+        assert g.last_gridding_kernel() == abi.KERNEL_TILED
+        np.testing.assert_allclose(g.grid_weights(), o.weights, rtol=1e-12)
+        res = fut.get()
+        grid = g.grid_values()
+        if precision == abi.PRECISION_FP64:
+            assert np.mean(np.all(res["vis"] == exp["vis"], axis=1)) > 0.99, k
+            o2 = oracle_for(O, job, False)
+            o2.grid_visibilities(res)
+            assert rel_norm(grid, o2.grid) <= 1e-12, k
+        else:
+            assert rel_norm(res["vis"], exp["vis"]) <= 1e-6, k
+        assert rel_norm(grid, o.grid) <= 1e-6, k
     for g in gs:
         g.close()
 
