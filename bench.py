@@ -442,8 +442,8 @@ def run_batch(args):
     drawn from {8, 16, 32, 64} at oversampling 64; mixed form.  One step
     grids every job's batch: the jobs of each polarization count go to one
     hpgb_grid_visibilities_batch call, which takes one persistent tiled
-    launch per support class of its gridders (nine launches at most here),
-    device-resident inputs.  The same step is timed with one call per job
+    launch per group of its gridders with the same CF support class and
+    tile side, device-resident inputs.  The same step is timed with one call per job
     (one tiled launch each) beside it.  Prints one JSON line: Mvis/s of both, and the
     batched launches' HBM roofline (records + CF slices once per visibility
     + grid read/write per job)."""
@@ -485,7 +485,7 @@ def run_batch(args):
         del vis
     torch.cuda.empty_cache()
     # one batched call per polarization class (the library splits each by
-    # the gridders' widest CF into one launch per support class)
+    # the gridders' widest CF and own tile side into launches)
     classes = {}
     for job in jobs:
         classes.setdefault(job["npol"], []).append(job)
@@ -530,13 +530,13 @@ def run_batch(args):
     def kernel_ms(cls):
         """Summed CUDA-event time of the tiled launches recorded since the
         last call, over the class's gridders (a batched call records its
-        launches on its first gridders: one per support class, which may
-        overlap)."""
-        tot = 0.0
+        launches on the first gridders of its groups; they may overlap)."""
+        tot, launches = 0.0, 0
         for j in cls:
             ms, n = j["g"].tiled_kernel_time()
             tot += ms
-        return tot
+            launches += n
+        return tot, launches
 
     for k, cls in classes.items():
         one = {k: cls}
@@ -544,7 +544,9 @@ def run_batch(args):
             j["g"].profile_tiled_kernel(True)
         kernel_ms(cls)
         mb = timed(lambda: batched(one))
-        kb = kernel_ms(cls) / (args.steps + args.warmup)
+        kb, nl = kernel_ms(cls)
+        kb /= args.steps + args.warmup
+        nl //= args.steps + args.warmup
         for j in cls:
             j["g"].profile_tiled_kernel(False)
         # (the per-job launches' event times are not summed: a launch on
@@ -555,7 +557,8 @@ def run_batch(args):
         per_class[f"{k}pol"] = {"jobs": len(cls),
                                 "vis": sum(j["nvis"] for j in cls),
                                 "batched_ms": mb, "per_job_ms": ms,
-                                "batched_kernel_ms_sum": kb}
+                                "batched_kernel_ms_sum": kb,
+                                "batched_launches": nl}
     for job in jobs:
         job["g"].set_gridding_kernel(abi.KERNEL_TILED)
     ms_single = timed(per_job)
@@ -574,10 +577,8 @@ def run_batch(args):
                    "batch_calls": len(classes),
                    "jobs_per_call": {f"{k}pol": len(v)
                                      for k, v in classes.items()},
-                   "launches": len({(j["npol"],
-                                     0 if j["max_support"] <= 16 else
-                                     1 if j["max_support"] <= 32 else 2)
-                                    for j in jobs})},
+                   "launches": sum(c["batched_launches"]
+                                   for c in per_class.values())},
         "per_class": per_class,
         "per_job_launches": {"value": total_vis / (ms_single * 1e-3) / 1e6,
                              "ms_per_step": ms_single},

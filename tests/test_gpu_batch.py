@@ -6,7 +6,8 @@ with two cubes), one to four CF groups with supports 4..16 (and 24 for
 some, so that the batch spans two support classes, which take a launch
 each on forked streams) at oversampling 8, batches of 0..5000
 visibilities, two polarizations with a diagonal Mueller matrix; a second
-set reaches support 64 (three support classes).  Tolerances as in the single-gridder parity tests:
+set reaches support 64 (three support classes).  Gridders of a batch are
+split into launches by support class and by their own plan's tile side.  Tolerances as in the single-gridder parity tests:
 FP64 gridding 1e-12; mixed 1e-6; FP64 degrid+grid residuals at least 99%
 bit-exact, and the grid within 1e-12 of the oracle's gridding of the
 device's residuals.
@@ -124,7 +125,8 @@ def test_batch_matches_oracle(gpu, oracle_lib, precision, comp, degrid):
 def make_wide_jobs(seed=5):
     """Gridders whose widest CFs reach support 64 (65 taps: the launch of
     that support class takes a two- or three-part CF ring) beside ones
-    whose widest are 32 and 16 (three support classes, three launches),
+    whose widest are 32 and 16 (three support classes, a launch or more
+    each),
     two polarizations, diagonal Mueller."""
     rng = np.random.default_rng(seed)
     jobs = []
