@@ -96,9 +96,9 @@ struct TiledParams {
   unsigned* status;
   const BatchJob* jobs;  // batched launches: the gridders' job table
   unsigned long long wait_limit_ns;  // bound of every wait in the kernel
-  // test hook: CTA 0 never issues the copies of this visibility (its ring
-  // position in CTA 0's sequence), so that the waits for them run out; -1:
-  // none
+  // test hook: the CTA of row 0 that takes this visibility (its position in
+  // the tile-sorted batch; of the first gridder in a batched launch) never
+  // issues its copies, so that the waits for them run out; -1: none
   long long withhold_vis;
 };
 
@@ -580,15 +580,18 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       run_dst[u] = p.run_dst[row][u];
     }
     const bool cf_needed = exchange || p.do_grid;
+    // the withholding test hook applies to the current pass (row 0, the
+    // first gridder's passes)
+    bool hook_job = false;
     // the copies of one visibility into slot s (one thread); jdescs, jcf:
     // the descriptors and CF of the pass's gridder (read from the job table
     // once per pass in a batched launch)
     auto issue = [&](const TileDesc* jdescs, const float2* jcf, int s,
                      int roff, long long off, int pstride, int dindex,
                      uint32_t qv) {
-      // test hook: CTA 0 never issues the copies of one visibility, so that
-      // the waits for them run out (the slot's phase never completes)
-      if (blockIdx.x == 0 && (long long)qv == p.withhold_vis) return;
+      // test hook: row 0 never issues the copies of one visibility, so
+      // that the waits for them run out (the slot's phase never completes)
+      if (hook_job && (long long)dindex == p.withhold_vis) return;
       const uint32_t pbytes = uint32_t(pstride) * 8u;
       const uint32_t need = cf_needed ? uint32_t(nplanes) * pbytes : 0u;
       ring_off[s] = roff;
@@ -616,6 +619,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       for (unsigned c = cid; c < nchunks; c += ncl) {
         const int count = p.chunks[c].count;
         const int cjob = BATCH ? p.chunks[c].pad : 0;
+        hook_job = p.withhold_vis >= 0 && row == 0 && cjob == 0;
         const TileDesc* jdescs = HPGB_JOB(BATCH, p, cjob, descs);
         const float2* jcf = HPGB_JOB(BATCH, p, cjob, cf);
 
@@ -638,6 +642,7 @@ tiled_kernel(const __grid_constant__ TiledParams p,
       unsigned long long tail = 0;      // ring bytes released (monotonic)
       for (unsigned c = cid; c < nchunks; c += ncl) {
         const Chunk ch = p.chunks[c];
+        hook_job = p.withhold_vis >= 0 && row == 0 && (!BATCH || ch.pad == 0);
         const TileDesc* jdescs = HPGB_JOB(BATCH, p, ch.pad, descs);
         const float2* jcf = HPGB_JOB(BATCH, p, ch.pad, cf);
         const SliceRef* jsrefs = HPGB_JOB(BATCH, p, ch.pad, srefs);

@@ -402,9 +402,10 @@ class Gridder:
         check(load().hpgb_set_wait_limit(self._h, float(seconds)))
 
     def debug_withhold_copy(self, visibility):
-        """Test hook: the first CTA of later tiled launches never issues the
-        copies of the visibility at this position of its sequence (-1:
-        none), so that the kernel takes its wait-timeout path."""
+        """Test hook: in later tiled launches, the grid-row-0 CTA that takes
+        the visibility at this position of the tile-sorted batch never
+        issues its copies (-1: none), so that the kernel takes its
+        wait-timeout path."""
         check(load().hpgb_debug_withhold_copy(self._h, int(visibility)))
 
     def last_gridding_kernel(self):

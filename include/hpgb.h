@@ -430,10 +430,11 @@ HPGB_API int hpgb_grid_visibilities_batch(
  * incomplete, and the gridder stays usable. */
 HPGB_API int hpgb_set_wait_limit(hpgb_gridder* gridder, double seconds);
 
-/* Test hook, no counterpart in the reference: the first CTA of the next
- * tiled launches never issues the bulk copies of the visibility at this
- * position of its sequence (-1: none), so that the waits for them run out
- * and the kernel takes its timeout path.  For tests of that path only. */
+/* Test hook, no counterpart in the reference: in the next tiled launches,
+ * the CTA of grid row 0 that takes the visibility at this position of the
+ * tile-sorted batch (of the first gridder, in a batched launch) never
+ * issues its bulk copies (-1: none), so that the waits for them run out and
+ * the kernel takes its timeout path.  For tests of that path only. */
 HPGB_API int hpgb_debug_withhold_copy(hpgb_gridder* gridder,
                                       long long visibility);
 

@@ -3,8 +3,8 @@ with an error status that the next fence reports, and the gridder stays
 usable.
 
 The failure is made on the host side of the kernel's contract, never by a
-fault: a test hook tells the first CTA not to issue the bulk copies of one
-visibility, so the mbarrier phase that announces them never completes (a
+fault: a test hook tells the grid-row-0 CTA that takes one visibility (a
+position in the tile-sorted batch) not to issue its bulk copies, so the mbarrier phase that announces them never completes (a
 flag that nothing sets).  With a 20 ms wait limit the waiting warps give up,
 set the CTA's abort flag, and every role winds down through its barriers;
 the peers of the cluster give up on that CTA's partial sums the same way.
