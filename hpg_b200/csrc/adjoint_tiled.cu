@@ -342,7 +342,7 @@ Status linear_op_tiled(hpgb_gridder* g, const void* d_vis, size_t n, int op,
   const int nty = (int(g->grid_size[1]) + T - 1) / T;
   TilePrep prep;
   HPGB_TRY(prepare_tiles(g, const_cast<void*>(d_vis), n, T, ntx, nty,
-                         kAdjChunk, &prep));
+                         kAdjChunk, &prep, nullptr, false));
   AdjParams p{};
   p.nx = int(g->grid_size[0]);
   p.ny = int(g->grid_size[1]);

@@ -8,13 +8,18 @@
 //                         compute_vis_coord) -> key = (cube, tile row, tile
 //                         col) of the tile holding the footprint origin;
 //                         histogram of keys
-//   2. cub radix sort     stable sort of (key, visibility index)
+//   2. cub radix sort     stable sort of (key, visibility index); the key's
+//                         low bits are the footprint's size class
 //   3. scans + chunks     tile starts; work chunks of <= kChunkVis visibilities
-//   4. tile_desc_kernel   one 256-byte descriptor per visibility in sorted
-//                         order (tile-relative footprint origin, phasor,
-//                         phase screen, degridding normaliser and grid-row
+//   4. tile_desc_kernel   one 256-byte descriptor per visibility
+//                         (tile-relative footprint origin, phasor, phase
+//                         screen, degridding normaliser and grid-row
 //                         weights from the per-slice CF sums, gridding
-//                         values) + the address of its CF slice
+//                         values) + the address of its CF slice, a tile's
+//                         visibilities interleaved large/small
+//                         (tile_order_source: measured 2.8% faster in the
+//                         mixed form, 1.5% in the FP64 form, than input
+//                         order; sorted by size alone, 3% slower)
 //   5. tiled_kernel       persistent, one thread-block cluster per tile with
 //                         one CTA per grid row (Mueller row) r; 20 warps:
 //                         - two producer warps stream each visibility's
@@ -102,11 +107,16 @@ __global__ void tile_keys_kernel(const VisData<N>* vis, size_t n, GridGeom g,
   VisCoord vc;
   vis_coords(g, groups, vd.freq, vd.uvw, vd.grid_cube, vd.cf_index,
              vd.cf_phase_gradient, vc);
-  unsigned key = unsigned(tg.ntiles);
+  unsigned key = unsigned(tg.ntiles) << tg.sbits;
   if (vc.in_grid) {
-    key = unsigned((vc.grid_cube * tg.nty + vc.grid_coord[1] / tg.T) * tg.ntx +
-                   vc.grid_coord[0] / tg.T);
-    atomicAdd(&counts[key], 1u);
+    const unsigned tile =
+        unsigned((vc.grid_cube * tg.nty + vc.grid_coord[1] / tg.T) * tg.ntx +
+                 vc.grid_coord[0] / tg.T);
+    // footprint size class in the key's low bits (cells / 128, capped)
+    const unsigned top = (1u << tg.sbits) - 1u;
+    const unsigned sc = min(top, unsigned(vc.taps[0] * vc.taps[1]) >> 7);
+    key = (tile << tg.sbits) | sc;
+    atomicAdd(&counts[tile], 1u);
   }
   keys[i] = key;
   order[i] = unsigned(i);
@@ -141,12 +151,18 @@ __global__ void tile_desc_kernel(const VisData<N>* vis, const unsigned* order,
                                  const unsigned* keys, size_t n, GridGeom g,
                                  const CFGroup* groups, TileGeom tg,
                                  const float2* cf_base, TileDesc* descs,
-                                 SliceRef* srefs) {
+                                 SliceRef* srefs, const unsigned* tstart,
+                                 const unsigned* tcount) {
   const size_t pidx = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
   if (pidx >= n) return;
-  const unsigned key = keys[pidx];
+  const unsigned key = keys[pidx] >> tg.sbits;  // the tile
   if (key >= unsigned(tg.ntiles)) return;
-  const unsigned i = order[pidx];
+  // the tile's visibilities are sorted by footprint size; descriptor
+  // position pidx takes the one tile_order_source picks
+  const unsigned t0 = tstart[key];
+  const unsigned r = unsigned(pidx) - t0;
+  const unsigned i =
+      order[t0 + (tg.interleave ? tile_order_source(r, tcount[key]) : r)];
   const VisData<N>& vd = vis[i];
   VisCoord vc;
   vis_coords(g, groups, vd.freq, vd.uvw, vd.grid_cube, vd.cf_index,
@@ -476,7 +492,8 @@ Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
 
 template <int N>
 Status prepare_tiles_n(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
-                       int nty, int K, TilePrep* out, cudaStream_t st) {
+                       int nty, int K, TilePrep* out, cudaStream_t st,
+                       bool interleave) {
   VisBuffers& vb = g->vb;
   const GridGeom geom = g->geom();
   const CFGroup* groups = g->cf.desc.as<const CFGroup>();
@@ -485,6 +502,9 @@ Status prepare_tiles_n(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
   tg.ntx = ntx;
   tg.nty = nty;
   tg.ntiles = tg.ntx * tg.nty * int(g->grid_size[3]);
+  // five bits of footprint size class below the tile while keys fit 32 bits
+  tg.interleave = interleave;
+  tg.sbits = interleave && (unsigned(tg.ntiles) + 1u) <= (1u << 27) ? 5 : 0;
   const int ntiles = tg.ntiles;
   const size_t max_chunks = n / K + size_t(ntiles) + 1;
   // scratch
@@ -505,7 +525,7 @@ Status prepare_tiles_n(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
                                                 n * sizeof(TileDesc));
   // CUB scratch sizing
   int end_bit = 1;
-  while ((1ll << end_bit) <= (long long)ntiles) ++end_bit;
+  while ((1ll << end_bit) <= ((long long)ntiles << tg.sbits)) ++end_bit;
   size_t sort_bytes = 0, scan_bytes = 0;
   cub::DoubleBuffer<unsigned> kbuf(vb.keys.as<unsigned>(), vb.keys_alt.as<unsigned>());
   cub::DoubleBuffer<unsigned> vbuf(vb.order.as<unsigned>(), vb.order_alt.as<unsigned>());
@@ -542,7 +562,8 @@ Status prepare_tiles_n(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
   ++g->launches;
   tile_desc_kernel<N><<<blocks, 256, 0, st>>>(
       static_cast<const VisData<N>*>(d_vis), vbuf.Current(), kbuf.Current(), n,
-      geom, groups, tg, g->cf.data.as<const float2>(), descs, srefs);
+      geom, groups, tg, g->cf.data.as<const float2>(), descs, srefs, tstart,
+      counts);
   HPGB_CUDA_TRY(cudaGetLastError());
   ++g->launches;
 
@@ -559,7 +580,7 @@ Status grid_tiled_n(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
                     const Plan& plan, bool mixed) {
   TilePrep prep;
   HPGB_TRY(prepare_tiles_n<N>(g, d_vis, n, plan.T, plan.p.ntx, plan.p.nty,
-                              plan.K, &prep, g->stream));
+                              plan.K, &prep, g->stream, true));
   VisBuffers& vb = g->vb;
   TileDesc* descs = const_cast<TileDesc*>(prep.descs);
   SliceRef* srefs = const_cast<SliceRef*>(prep.srefs);
@@ -589,13 +610,14 @@ Status grid_tiled_n(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
 }  // namespace
 
 Status prepare_tiles(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
-                     int nty, int K, TilePrep* out, cudaStream_t st) {
+                     int nty, int K, TilePrep* out, cudaStream_t st,
+                     bool interleave) {
   if (!st) st = g->stream;
   switch (g->npol) {
-    case 1: return prepare_tiles_n<1>(g, d_vis, n, T, ntx, nty, K, out, st);
-    case 2: return prepare_tiles_n<2>(g, d_vis, n, T, ntx, nty, K, out, st);
-    case 3: return prepare_tiles_n<3>(g, d_vis, n, T, ntx, nty, K, out, st);
-    case 4: return prepare_tiles_n<4>(g, d_vis, n, T, ntx, nty, K, out, st);
+    case 1: return prepare_tiles_n<1>(g, d_vis, n, T, ntx, nty, K, out, st, interleave);
+    case 2: return prepare_tiles_n<2>(g, d_vis, n, T, ntx, nty, K, out, st, interleave);
+    case 3: return prepare_tiles_n<3>(g, d_vis, n, T, ntx, nty, K, out, st, interleave);
+    case 4: return prepare_tiles_n<4>(g, d_vis, n, T, ntx, nty, K, out, st, interleave);
     default: return Status::err(HPGB_ERROR_OTHER, "bad polarization count");
   }
 }

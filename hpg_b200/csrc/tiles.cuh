@@ -3,10 +3,11 @@
 // (adjoint_tiled.cu).
 //
 // A batch is sorted by the uv tile (T x T cells of footprint origins, per
-// grid cube) that holds each visibility's footprint origin; each tile's
-// visibilities are cut into passes ("chunks") of at most K; every visibility
-// in sorted order gets a 256-byte descriptor of what the kernels need and
-// the offset of its CF slice.
+// grid cube) that holds each visibility's footprint origin, and within a
+// tile by footprint size, then interleaved large/small (tile_order_source);
+// each tile's visibilities are cut into passes ("chunks") of at most K;
+// every visibility in that order gets a 256-byte descriptor of what the
+// kernels need and the offset of its CF slice.
 #pragma once
 
 #include "gridder.cuh"
@@ -44,7 +45,23 @@ struct Chunk {
 
 struct TileGeom {
   int T, ntx, nty, ntiles;  // ntiles = ncube * nty * ntx (also the invalid key)
+  // bits of the sort key below the tile: the footprint's size class (0 when
+  // the key has no room, or without interleaving)
+  int sbits;
+  int interleave;  // order a tile's visibilities by tile_order_source
 };
+
+// Order of a tile's visibilities: sorted by footprint size, then taken as
+// large, small, small, large, large, small, ... (position r of the tile's n
+// takes sorted position n - 1 - r/2 when large, r/2 when small).  Each
+// consecutive pair holds one large and one small footprint, so the CF ring
+// keeps a mix of large and small parts in flight, and each of two groups
+// that take alternate visibilities alternates between large and small.
+__host__ __device__ inline unsigned tile_order_source(unsigned r, unsigned n) {
+  const unsigned k = r >> 1;
+  const bool large = ((k & 1u) == 0u) == ((r & 1u) == 0u);
+  return large ? n - 1u - k : k;
+}
 
 // where prepare_tiles leaves its results (the gridder's batch buffers)
 struct TilePrep {
@@ -58,7 +75,13 @@ struct TilePrep {
 // Sorts the batch d_vis (n VisData<npol> records in device memory) into
 // tiles of T x T origins, ntx x nty tiles per grid cube, passes of at most
 // K visibilities; all on stream st (the gridder's stream when null).
+// interleave: a tile's visibilities in tile_order_source's large/small
+// order (the tiled gridding kernel, whose pipeline runs best on a mix of
+// footprint sizes); otherwise in batch order (the tiled linear operators,
+// whose warps take every 16th visibility of a pass: a periodic size pattern
+// would give some warps only large footprints).
 Status prepare_tiles(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
-                     int nty, int K, TilePrep* out, cudaStream_t st = nullptr);
+                     int nty, int K, TilePrep* out, cudaStream_t st = nullptr,
+                     bool interleave = true);
 
 }  // namespace hpgb
