@@ -165,10 +165,10 @@ def make_workload(args, seed_offset, device):
 
 # DRAM bytes (read + write) of one tiled-kernel launch, from an ncu capture
 # of 200k visibilities of this workload at CF oversampling 64 (mixed form:
-# 15.77 GB, of which 0.67 GB are the model and grid passes; FP64 form:
+# 15.75 GB, of which 0.67 GB are the model and grid passes; FP64 form:
 # 16.04 GB, 0.81 GB), scaled to a launch by the visibility count.
-TRAFFIC_PER_VIS_MIXED = (15.769e9 - 0.671e9) / 200_000
-TRAFFIC_PER_VIS_FP64 = (16.041e9 - 0.805e9) / 200_000
+TRAFFIC_PER_VIS_MIXED = (15.754e9 - 0.671e9) / 200_000
+TRAFFIC_PER_VIS_FP64 = (16.036e9 - 0.805e9) / 200_000
 
 
 def kernel_traffic(form, nvis, grid_elems):
