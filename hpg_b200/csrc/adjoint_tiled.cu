@@ -3,7 +3,12 @@
 // differentiable-imaging workloads: degridding D (src/hpg_core.hpp:580-682)
 // and its adjoint, gridding G (:791-886) and its adjoint.
 //
-// The batch is sorted into uv tiles of T x T footprint origins (tiles.cuh).
+// The batch is sorted into uv tiles of T x T footprint origins (tiles.cuh),
+// a tile's visibilities in descending footprint size with every other block
+// of 16 reversed (kOrderSnake16): the 16 warps of a CTA take visibilities
+// r = warp, warp + 16, ... of a pass and meet at its end, so their shares
+// of footprint cells come out nearly even (measured at 10M visibilities:
+// 43.4 against 35.2 Mvis/s per gradient step in batch order).
 // A persistent CTA takes one tile pass at a time from a device work counter
 // and keeps the pass's grid region -- R x R cells (R = T + taps - 1) of
 // every grid row -- in shared memory as FP64:
@@ -342,7 +347,7 @@ Status linear_op_tiled(hpgb_gridder* g, const void* d_vis, size_t n, int op,
   const int nty = (int(g->grid_size[1]) + T - 1) / T;
   TilePrep prep;
   HPGB_TRY(prepare_tiles(g, const_cast<void*>(d_vis), n, T, ntx, nty,
-                         kAdjChunk, &prep, nullptr, false));
+                         kAdjChunk, &prep, nullptr, kOrderSnake16));
   AdjParams p{};
   p.nx = int(g->grid_size[0]);
   p.ny = int(g->grid_size[1]);

@@ -161,8 +161,7 @@ __global__ void tile_desc_kernel(const VisData<N>* vis, const unsigned* order,
   // position pidx takes the one tile_order_source picks
   const unsigned t0 = tstart[key];
   const unsigned r = unsigned(pidx) - t0;
-  const unsigned i =
-      order[t0 + (tg.interleave ? tile_order_source(r, tcount[key]) : r)];
+  const unsigned i = order[t0 + tile_order_source(r, tcount[key], tg.order)];
   const VisData<N>& vd = vis[i];
   VisCoord vc;
   vis_coords(g, groups, vd.freq, vd.uvw, vd.grid_cube, vd.cf_index,
@@ -493,7 +492,7 @@ Status launch_tiled(hpgb_gridder* g, const TiledParams& p, int smem,
 template <int N>
 Status prepare_tiles_n(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
                        int nty, int K, TilePrep* out, cudaStream_t st,
-                       bool interleave) {
+                       int order) {
   VisBuffers& vb = g->vb;
   const GridGeom geom = g->geom();
   const CFGroup* groups = g->cf.desc.as<const CFGroup>();
@@ -503,8 +502,8 @@ Status prepare_tiles_n(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
   tg.nty = nty;
   tg.ntiles = tg.ntx * tg.nty * int(g->grid_size[3]);
   // five bits of footprint size class below the tile while keys fit 32 bits
-  tg.interleave = interleave;
-  tg.sbits = interleave && (unsigned(tg.ntiles) + 1u) <= (1u << 27) ? 5 : 0;
+  tg.sbits = (unsigned(tg.ntiles) + 1u) <= (1u << 27) ? 5 : 0;
+  tg.order = tg.sbits ? order : kOrderBatch;
   const int ntiles = tg.ntiles;
   const size_t max_chunks = n / K + size_t(ntiles) + 1;
   // scratch
@@ -580,7 +579,7 @@ Status grid_tiled_n(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
                     const Plan& plan, bool mixed) {
   TilePrep prep;
   HPGB_TRY(prepare_tiles_n<N>(g, d_vis, n, plan.T, plan.p.ntx, plan.p.nty,
-                              plan.K, &prep, g->stream, true));
+                              plan.K, &prep, g->stream, kOrderPairs));
   VisBuffers& vb = g->vb;
   TileDesc* descs = const_cast<TileDesc*>(prep.descs);
   SliceRef* srefs = const_cast<SliceRef*>(prep.srefs);
@@ -611,13 +610,13 @@ Status grid_tiled_n(hpgb_gridder* g, void* d_vis, size_t n, unsigned flags,
 
 Status prepare_tiles(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
                      int nty, int K, TilePrep* out, cudaStream_t st,
-                     bool interleave) {
+                     int order) {
   if (!st) st = g->stream;
   switch (g->npol) {
-    case 1: return prepare_tiles_n<1>(g, d_vis, n, T, ntx, nty, K, out, st, interleave);
-    case 2: return prepare_tiles_n<2>(g, d_vis, n, T, ntx, nty, K, out, st, interleave);
-    case 3: return prepare_tiles_n<3>(g, d_vis, n, T, ntx, nty, K, out, st, interleave);
-    case 4: return prepare_tiles_n<4>(g, d_vis, n, T, ntx, nty, K, out, st, interleave);
+    case 1: return prepare_tiles_n<1>(g, d_vis, n, T, ntx, nty, K, out, st, order);
+    case 2: return prepare_tiles_n<2>(g, d_vis, n, T, ntx, nty, K, out, st, order);
+    case 3: return prepare_tiles_n<3>(g, d_vis, n, T, ntx, nty, K, out, st, order);
+    case 4: return prepare_tiles_n<4>(g, d_vis, n, T, ntx, nty, K, out, st, order);
     default: return Status::err(HPGB_ERROR_OTHER, "bad polarization count");
   }
 }

@@ -4,7 +4,7 @@
 //
 // A batch is sorted by the uv tile (T x T cells of footprint origins, per
 // grid cube) that holds each visibility's footprint origin, and within a
-// tile by footprint size, then interleaved large/small (tile_order_source);
+// tile by footprint size, then reordered (tile_order_source);
 // each tile's visibilities are cut into passes ("chunks") of at most K;
 // every visibility in that order gets a 256-byte descriptor of what the
 // kernels need and the offset of its CF slice.
@@ -46,21 +46,40 @@ struct Chunk {
 struct TileGeom {
   int T, ntx, nty, ntiles;  // ntiles = ncube * nty * ntx (also the invalid key)
   // bits of the sort key below the tile: the footprint's size class (0 when
-  // the key has no room, or without interleaving)
+  // the key has no room, or in batch order)
   int sbits;
-  int interleave;  // order a tile's visibilities by tile_order_source
+  int order;  // TileOrder: how a tile's visibilities are ordered
 };
 
-// Order of a tile's visibilities: sorted by footprint size, then taken as
-// large, small, small, large, large, small, ... (position r of the tile's n
-// takes sorted position n - 1 - r/2 when large, r/2 when small).  Each
-// consecutive pair holds one large and one small footprint, so the CF ring
-// keeps a mix of large and small parts in flight, and each of two groups
-// that take alternate visibilities alternates between large and small.
-__host__ __device__ inline unsigned tile_order_source(unsigned r, unsigned n) {
-  const unsigned k = r >> 1;
-  const bool large = ((k & 1u) == 0u) == ((r & 1u) == 0u);
-  return large ? n - 1u - k : k;
+// How a tile's visibilities are ordered (each from the tile's visibilities
+// sorted by footprint size, ascending; position r of the tile's n takes the
+// sorted position tile_order_source gives):
+//  - kOrderBatch: as in the batch;
+//  - kOrderPairs (the tiled gridding kernel): large, small, small, large,
+//    large, small, ... (n - 1 - r/2 when large, r/2 when small): each
+//    consecutive pair holds one large and one small footprint, so the CF
+//    ring keeps a mix of large and small parts in flight, and each of two
+//    groups that take alternate visibilities alternates between them;
+//  - kOrderSnake16 (the tiled linear operators, whose 16 warps take
+//    visibilities r = warp, warp + 16, ... of a pass and meet at its end):
+//    descending size, every other block of 16 reversed, so that each warp's
+//    share of the footprints comes out nearly even.
+enum TileOrder : int { kOrderBatch = 0, kOrderPairs = 1, kOrderSnake16 = 2 };
+
+__host__ __device__ inline unsigned tile_order_source(unsigned r, unsigned n,
+                                                      int order) {
+  if (order == kOrderPairs) {
+    const unsigned k = r >> 1;
+    const bool large = ((k & 1u) == 0u) == ((r & 1u) == 0u);
+    return large ? n - 1u - k : k;
+  }
+  if (order == kOrderSnake16) {
+    const unsigned b = r >> 4, i = r & 15u;
+    const unsigned m = n - (b << 4) < 16u ? n - (b << 4) : 16u;  // block size
+    const unsigned d = (b << 4) + ((b & 1u) ? m - 1u - i : i);  // descending
+    return n - 1u - d;
+  }
+  return r;
 }
 
 // where prepare_tiles leaves its results (the gridder's batch buffers)
@@ -75,13 +94,11 @@ struct TilePrep {
 // Sorts the batch d_vis (n VisData<npol> records in device memory) into
 // tiles of T x T origins, ntx x nty tiles per grid cube, passes of at most
 // K visibilities; all on stream st (the gridder's stream when null).
-// interleave: a tile's visibilities in tile_order_source's large/small
-// order (the tiled gridding kernel, whose pipeline runs best on a mix of
-// footprint sizes); otherwise in batch order (the tiled linear operators,
-// whose warps take every 16th visibility of a pass: a periodic size pattern
-// would give some warps only large footprints).
+// order: TileOrder of a tile's visibilities (kOrderPairs for the tiled
+// gridding kernel, whose pipeline runs best on a mix of footprint sizes;
+// kOrderSnake16 for the tiled linear operators).
 Status prepare_tiles(hpgb_gridder* g, void* d_vis, size_t n, int T, int ntx,
                      int nty, int K, TilePrep* out, cudaStream_t st = nullptr,
-                     bool interleave = true);
+                     int order = kOrderPairs);
 
 }  // namespace hpgb
