@@ -228,15 +228,17 @@ def test_tiled_operators_equal_direct(gpu):
     gd.close()
 
 
+@pytest.mark.parametrize("grad", [0.2, None], ids=["screen", "no-screen"])
 @pytest.mark.parametrize("npol,expect", [(1, abi.KERNEL_TILED),
                                          (2, abi.KERNEL_TILED),
                                          (4, abi.KERNEL_DIRECT)])
-def test_wide_support_dot_products(gpu, npol, expect):
+def test_wide_support_dot_products(gpu, npol, expect, grad):
     """Supports 8..64 (9..65 taps), diagonal Mueller, as in the
-    differentiable workload: both dot-product identities.  One or two grid
-    rows take the tiled operators; four rows of FP64 regions for 65 taps do
-    not fit shared memory, and the automatic choice takes the per-visibility
-    kernels."""
+    differentiable workload: both dot-product identities, with phase screens
+    and without (the workload's case: the operators' cell loops without a
+    screen take more cells per lane).  One or two grid rows take the tiled
+    operators; four rows of FP64 regions for 65 taps do not fit shared
+    memory, and the automatic choice takes the per-visibility kernels."""
     import torch
     from hpg_b200 import autograd as ag
     rng = np.random.default_rng(50 + npol)
@@ -247,7 +249,7 @@ def test_wide_support_dot_products(gpu, npol, expect):
     mi = [[r if c == r else -1 for c in range(npol)] for r in range(npol)]
     vis = workloads.visibilities(2000, npol, gs, (0.05, 0.05), 1.4e9, rng,
                                  disk=0.3, w_frac=0.3, ngroups=len(supports),
-                                 grad=0.2)
+                                 grad=grad)
     g = Gridder.create(0, 0, len(vis), None, gs, (0.05, 0.05), mi, mi)
     g.set_gridding_kernel(abi.KERNEL_AUTO)
     g.set_convolution_function(CFArray(8, ext, vals))
@@ -265,4 +267,23 @@ def test_wide_support_dot_products(gpu, npol, expect):
         assert abs(lhs) > 0
         assert abs(lhs - rhs) / abs(lhs) <= 1e-10
         assert g.last_gridding_kernel() == expect
+    if expect == abi.KERNEL_TILED:
+        # the tiled operators and their adjoints against the per-visibility
+        # kernels: the same FP64 arithmetic in another order (1e-12)
+        gd = Gridder.create(0, 0, len(vis), None, gs, (0.05, 0.05), mi, mi)
+        gd.set_gridding_kernel(abi.KERNEL_DIRECT)
+        gd.set_convolution_function(CFArray(8, ext, vals))
+        for op, arg, cot in ((ag.Degrid, x, y), (ag.Grid, y, x)):
+            a = op.apply(arg, g, dvis)
+            b = op.apply(arg, gd, dvis)
+            assert torch.linalg.norm(a - b) / torch.linalg.norm(b) <= 1e-12
+            ar = arg.clone().requires_grad_(True)
+            op.apply(ar, g, dvis).backward(cot)
+            br = arg.clone().requires_grad_(True)
+            op.apply(br, gd, dvis).backward(cot)
+            assert (torch.linalg.norm(ar.grad - br.grad) /
+                    torch.linalg.norm(br.grad)) <= 1e-12
+        assert g.last_gridding_kernel() == abi.KERNEL_TILED
+        assert gd.last_gridding_kernel() == abi.KERNEL_DIRECT
+        gd.close()
     g.close()
