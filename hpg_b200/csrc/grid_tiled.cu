@@ -395,6 +395,12 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
   // footprints covers.  kMinRingParts is the least the plan takes.
   constexpr int kMinRingParts = 2;
   constexpr size_t kMinVisPerTile = 32;
+  // the ring depth that few visibilities per tile still keep when it fits:
+  // two parts are for CF slices too wide for three (measured on a 2048^2
+  // grid with dense Mueller: at 50k visibilities 2.21 -> 1.58 ms mixed,
+  // 2.76 -> 1.95 ms FP64; at 200k 7.51 -> 5.73 ms in the compensated form,
+  // whose four tiles leave the least room)
+  constexpr int kFewVisParts = 3;
   const hpgb_tiled_plan& tp = g->tplan;
   const bool fixed = tp.ring_parts > 0;
   const int m_hi = fixed ? tp.ring_parts : 5;
@@ -420,7 +426,7 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
       R = tp.tile_side;
     }
     if (R - taps + 1 < 4) continue;
-    if (!fixed && m > m_lo) {
+    if (!fixed && m > std::max(m_lo, kFewVisParts)) {
       // tiles of the batch (of every gridder of a batched launch, each
       // with the largest tile its own CF allows in the region)
       auto tiles = [R](size_t nx, size_t ny, size_t ncube, int t) {
