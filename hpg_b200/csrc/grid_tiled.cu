@@ -401,6 +401,7 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
   // 2.76 -> 1.95 ms FP64; at 200k 7.51 -> 5.73 ms in the compensated form,
   // whose four tiles leave the least room)
   constexpr int kFewVisParts = 3;
+  constexpr int kSideTrim = 6;
   const hpgb_tiled_plan& tp = g->tplan;
   const bool fixed = tp.ring_parts > 0;
   const int m_hi = fixed ? tp.ring_parts : 5;
@@ -426,6 +427,15 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
       R = tp.tile_side;
     }
     if (R - taps + 1 < 4) continue;
+    // automatic plans at four parts or fewer: a side kSideTrim cells below
+    // the largest, whose freed bytes deepen the ring (the autotuner picks 4
+    // to 12 cells below there on the 2048^2 full-polarization workload;
+    // measured with the automatic plan: 1M visibilities mixed 22.95 -> 19.22
+    // ms, 200k FP64 6.71 -> 6.13 ms, the batched benchmark 71.7 -> 74.2
+    // Mvis/s), while tile strides stay >= 8
+    if (!fixed && tp.tile_side <= 0 && m <= 4 &&
+        R - kSideTrim - taps + 1 >= 8)
+      R -= kSideTrim;
     if (!fixed && m > std::max(m_lo, kFewVisParts)) {
       // tiles of the batch (of every gridder of a batched launch, each
       // with the largest tile its own CF allows in the region)
