@@ -427,15 +427,14 @@ Plan make_plan(const hpgb_gridder* g, unsigned flags, bool mixed,
       R = tp.tile_side;
     }
     if (R - taps + 1 < 4) continue;
-    // automatic plans at four parts or fewer: a side kSideTrim cells below
-    // the largest, whose freed bytes deepen the ring (the autotuner picks 4
-    // to 12 cells below there on the 2048^2 full-polarization workload;
-    // measured with the automatic plan: 1M visibilities mixed 22.95 -> 19.22
-    // ms, 200k FP64 6.71 -> 6.13 ms, the batched benchmark 71.7 -> 74.2
-    // Mvis/s), while tile strides stay >= 8
-    if (!fixed && tp.tile_side <= 0 && m <= 4 &&
-        R - kSideTrim - taps + 1 >= 8)
-      R -= kSideTrim;
+    // automatic plans at four parts or fewer: a side up to kSideTrim cells
+    // below the largest, whose freed bytes deepen the ring (the autotuner
+    // picks 4 to 12 cells below there on the 2048^2 full-polarization
+    // workload; measured with the automatic plan: 1M visibilities mixed
+    // 22.95 -> 19.22 ms, 200k FP64 6.71 -> 6.13 ms, the batched benchmark
+    // 71.7 -> 74.2 Mvis/s), while tile strides stay >= 8
+    if (!fixed && tp.tile_side <= 0 && m <= 4)
+      R -= std::max(0, std::min(kSideTrim, (R - taps + 1 - 8) & ~1));
     if (!fixed && m > std::max(m_lo, kFewVisParts)) {
       // tiles of the batch (of every gridder of a batched launch, each
       // with the largest tile its own CF allows in the region)
